@@ -1,0 +1,303 @@
+#!/usr/bin/env python
+"""Benchmark of the OPW path on B200: full-size filtered OPW power Doppler.
+
+Workload (one "step" = one ensemble): 128 + 128 element RCA, 0.11 mm pitch,
+fs 20 MHz, f_demod 15 MHz, c 1540 m/s; complex64 IQ of 512 samples x 128
+channels x 11 angles (-10..10 deg) x 200 frames per aperture; a 128 x 256 x 128
+(x, z, y) grid over +-7 mm laterally and 4-12 mm in depth; full receive
+aperture.  A step packs both apertures, beamforms OPW IQ with power, forms the
+temporal Gram matrix, eigendecomposes it and reduces the clutter-filtered
+power Doppler (rank_start = 3).
+
+Metric: OPW samples/s, one sample = voxel x receive channel x angle x frame
+over both apertures (2.362e12 per step), plus filtered-PD ms per ensemble.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU (torchrun): one independent ensemble per rank (weak scaling, no
+data-path collective); rank 0 prints the JSON line with the max-over-ranks time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+NS, NC, NA, NT = 512, 128, 11, 200
+GRID_SHAPE = (128, 256, 128)
+PITCH = 0.11e-3
+FS, FD, C = 20e6, 15e6, 1540.0
+T_START = 4e-6
+RANK_START = 3
+
+
+def workload():
+    el = (np.arange(NC) - (NC - 1) / 2) * PITCH
+    angles = np.deg2rad(np.linspace(-10, 10, NA))
+    half = (NC - 1) / 2 * PITCH
+    grid = (np.linspace(-half, half, GRID_SHAPE[0]), np.linspace(4e-3, 12e-3, GRID_SHAPE[1]),
+            np.linspace(-half, half, GRID_SHAPE[2]))
+    return el, angles, grid
+
+
+def units_per_step() -> int:
+    return int(np.prod(GRID_SHAPE)) * 2 * NC * NA * NT
+
+
+CONFIG = {
+    "workload": "filtered OPW PD: RCA 128+128 el 0.11 mm, IQ 512x128x11x200 c64 per aperture, grid 128x256x128, "
+                "fs 20 MHz, f_demod 15 MHz, full aperture, SVD clutter filter rank_start=3",
+    "samples": NS, "channels": NC, "angles": NA, "frames": NT, "grid": list(GRID_SHAPE),
+    "l2": "inputs (2.3 GB packed channels, 6.7 GB IQ) are larger than L2; no flush",
+}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.path.open("w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self) -> dict:
+        rows = [r.split(", ") for r in self.path.read_text().splitlines() if r.count(",") >= 8]
+        self.path.unlink(missing_ok=True)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.strip() == "Active"})
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(rows[0][2]),
+                "samples": len(rows), "reasons": reasons}
+
+
+def peaks() -> dict:
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
+
+
+# ----------------------------------------------------------------- B200 arm --
+def run_b200(args, rank: int, world: int) -> dict | None:
+    import torch
+
+    from rcabeam_b200 import _lib, pipeline
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    el, angles, grid = workload()
+    from rcabeam_b200.sim import RCAGeometry
+
+    geom = RCAGeometry(el, el, c=C, fs=FS, f_demod=FD, fnumber=None)
+    plan = pipeline.FilteredOpw((NS, NC, NA, NT), angles, T_START, grid, geom, rank_start=RANK_START)
+    gen = torch.Generator(device=dev).manual_seed(1234 + rank)
+    scene = pipeline.synthetic_channels((NS, NC, NA, NT), generator=gen, device=dev)
+    rc, cr = scene
+    torch.cuda.synchronize()
+
+    def step():
+        plan.run(rc, cr)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    das_ms = []
+    with ClockSampler(dev.index) as clocks:
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(args.steps):
+            step()
+            das_ms.append(plan.last_das_event_ms)
+        stop.record()
+        torch.cuda.synchronize()
+    elapsed = start.elapsed_time(stop) / 1e3
+    das_ms = [plan.collect_das_ms(e) for e in das_ms]
+    if world > 1:
+        t = torch.tensor([elapsed], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        elapsed = float(t.item())
+        torch.distributed.barrier()
+    assert _lib.device_error() == 0
+    clock = clocks.summary()
+
+    # End to end through the public API: pinned host channels -> host filtered power.
+    host_rc = rc.cpu().pin_memory()
+    host_cr = cr.cpu().pin_memory()
+    plan.run_host(host_rc, host_cr)
+    torch.cuda.synchronize()
+    e_start, e_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_steps = max(1, min(args.steps, 3))
+    e_start.record()
+    for _ in range(e_steps):
+        out = plan.run_host(host_rc, host_cr)
+    e_stop.record()
+    torch.cuda.synchronize()
+    e2e = e_start.elapsed_time(e_stop) / 1e3 / e_steps
+
+    if rank != 0:
+        return None
+    units = units_per_step()
+    value = units * world * args.steps / elapsed / 1e9
+    das_s = statistics.median(das_ms) / 1e3
+    pk = peaks()
+    # Compulsory DAS bytes per launch: packed channels read + IQ written + power written.
+    das_bytes = 2 * NS * NC * NA * NT * 8 + int(np.prod(GRID_SHAPE)) * NT * 8 + int(np.prod(GRID_SHAPE)) * 8
+    smem_peak = 148 * 128 * (clock["sm_mhz"] or 1965.0) * 1e6 / 1e9
+    line = {
+        "metric": "OPW Gsamples/s (vox*ch*ang*frm), filtered PD", "value": round(value, 3), "unit": "Gsamples/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(elapsed / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (c64 IQ, f64 geometry, f64 Gram/eig/projection)",
+        "data": "synthetic seeded channel IQ (complex Gaussian speckle), full-size shapes", "config": CONFIG,
+        "filtered_pd_ms_per_ensemble": round(elapsed / args.steps * 1e3, 3),
+        "stages_ms": plan.stage_ms(),
+        "e2e": {"value": round(units / e2e / 1e9, 3), "unit": "Gsamples/s", "ms_per_ensemble": round(e2e * 1e3, 3),
+                "h2d_bytes_per_step": int(host_rc.numel() * 8 * 2),
+                "d2h_bytes_per_step": int(out.numel() * out.element_size())},
+        "roofline": {"bound": "hbm", "kernel": "opw_staged (DAS)", "achieved": round(das_bytes / das_s / 1e9, 2),
+                     "peak": pk.get("hbm_gbs"), "unit": "GB/s",
+                     "frac": round(das_bytes / das_s / 1e9 / pk.get("hbm_gbs", 6650.0), 5),
+                     "traffic": None, "das_ms": round(das_s * 1e3, 3),
+                     "note": "compulsory bytes; DAS is bound by shared-memory gathers, see gather_roofline"},
+        "gather_roofline": {"bound": "smem", "bytes_per_sample": 16, "achieved": round(units * 16 / das_s / 1e9, 1),
+                            "peak": round(smem_peak, 1), "unit": "GB/s",
+                            "frac": round(units * 16 / das_s / 1e9 / smem_peak, 4)},
+        "clocks": clock,
+        "gpu_launches": plan.launches_per_step() * args.steps,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, reference_arm=False)
+    return line
+
+
+# ------------------------------------------------------- CPU (oracle) arms --
+def _oracle_sample(seed: int, voxels: int):
+    """A bounded slice of the workload for the float64 CPU oracle: the first voxels of the grid."""
+    from oracle import das
+
+    el, angles, grid = workload()
+    rng = np.random.default_rng(seed)
+    shape = (NS, NC, NA, NT)
+    rc = (rng.standard_normal(shape, dtype=np.float32) + 1j * rng.standard_normal(shape, dtype=np.float32))
+    cr = (rng.standard_normal(shape, dtype=np.float32) + 1j * rng.standard_normal(shape, dtype=np.float32))
+    scan = das.scan_coords(grid)[:voxels].astype(np.float64)
+    return rc.astype(np.complex64), cr.astype(np.complex64), scan, el, angles
+
+
+def _oracle_chunk(payload):
+    from oracle import das
+
+    rc, cr, scan, el, angles = payload
+    iq = das.opw_iq(rc, cr, scan, el, el, angles, T_START, C, FS, FD, None)
+    return das.power_doppler(iq)
+
+
+def cpu_baseline(args, reference_arm: bool) -> dict:
+    """Time the float64 oracle port of the reference NumPy path on a bounded voxel sample."""
+    import multiprocessing as mp
+
+    cores = (os.cpu_count() or 1) if reference_arm else 1
+    voxels = args.cpu_voxels * cores
+    rc, cr, scan, el, angles = _oracle_sample(7, voxels)
+    chunks = np.array_split(scan, cores)
+    begin = time.perf_counter()
+    if cores > 1:
+        with mp.get_context("spawn").Pool(cores) as pool:
+            pool.map(_oracle_chunk, [(rc, cr, c, el, angles) for c in chunks])
+    else:
+        _oracle_chunk((rc, cr, scan, el, angles))
+    seconds = time.perf_counter() - begin
+    units = voxels * 2 * NC * NA * NT
+    return {"value": round(units / seconds / 1e9, 5), "unit": "Gsamples/s", "cores": cores, "kind": "port",
+            "sample": f"{voxels} voxels x 256 ch x 11 ang x 200 frm of the workload (DAS + OPW + PD, float64 NumPy "
+                      f"restatement of reference sim._delay_numpy), {seconds:.1f} s"}
+
+
+def run_reference(args, rank: int, world: int) -> dict | None:
+    if rank != 0:
+        return None
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(args, reference_arm=True)
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(args, reference_arm=True))
+    value = statistics.median(v["value"] for v in vals)
+    base = dict(vals[-1])
+    base["value"] = value
+    return {
+        "impl": "reference", "metric": "OPW Gsamples/s (vox*ch*ang*frm), filtered PD", "value": value,
+        "unit": "Gsamples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": CONFIG, "cpu_baseline": base,
+        "e2e": {"value": value, "unit": "Gsamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-voxels", type=int, default=192, help="oracle voxels per core for the CPU baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        if world > 1:
+            import datetime
+
+            import torch
+
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+            torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        line = run_b200(args, rank, world)
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,159 @@
+/* rcabeam C ABI -- B200 (sm_100a) implementation.
+ *
+ * Every declaration in the first part keeps the exact name, argument order,
+ * types and status semantics of the reference interface include/rcabeam.h of
+ * sdiebolt/rcabeam; the comment above each one cites the reference line it
+ * replaces.  Declarations under "Extensions" have no reference C counterpart:
+ * they expose the clutter filter (a CuPy module in the reference) and the
+ * device error word of the bounded-wait kernels.
+ *
+ * All pointers are device pointers unless stated otherwise.  Work is launched
+ * on the legacy default CUDA stream, as in the reference (rcabeam.h:200), and
+ * calls return once the work is enqueued.  Nothing here allocates device
+ * memory except the clutter-filter extensions, which say so.
+ */
+#pragma once
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* reference rcabeam.h:9-13 */
+typedef enum rcabeam_status {
+    RCABEAM_SUCCESS = 0,
+    RCABEAM_ERROR_CUDA = 1,
+    RCABEAM_ERROR_ARGUMENT = 2,
+} rcabeam_status;
+
+/* reference rcabeam.h:15 */
+const char* rcabeam_status_string(rcabeam_status status);
+
+/* ---- Per-frame entry points (reference rcabeam.h:17-182; core.cu). ------
+ * Single-frame channel layout is (samples, channels, angles) complex64;
+ * per-angle IQ is (voxels, angles, frames).  config 0 = RC, 1 = CR.
+ * f_number <= 0 keeps the full receive aperture. */
+
+/* reference rcabeam.h:17-23: out[v, t] = sum over angles of iq[v, a, t]. */
+rcabeam_status rcabeam_opw_device(const void* iq, void* out, size_t n_voxels, size_t n_angles, size_t n_frames);
+
+/* reference rcabeam.h:25-35: |mean_t (sum RC angles)(sum CR angles)^*|. */
+rcabeam_status rcabeam_xdoppler_pd_device(const void* iq, float* out, size_t n_voxels, size_t n_angles,
+                                          size_t n_frames, size_t rc_start, size_t rc_count, size_t cr_start,
+                                          size_t cr_count);
+
+/* reference rcabeam.h:37-47: mean_t |(sum sqrt RC)(sum sqrt CR)|^2. */
+rcabeam_status rcabeam_rc_fmas_pd_device(const void* iq, float* out, size_t n_voxels, size_t n_angles,
+                                         size_t n_frames, size_t rc_start, size_t rc_count, size_t cr_start,
+                                         size_t cr_count);
+
+/* reference rcabeam.h:49-65: per-angle DAS volumes out[v, a] of one frame. */
+rcabeam_status rcabeam_delay_rca_channels_device(const void* iq_ch, const float* scan_coords_m,
+                                                 const float* elements_m, const float* angles_rad,
+                                                 const float* t_start_s, void* out, size_t n_samples,
+                                                 size_t n_channels, size_t n_angles, size_t n_voxels, int config,
+                                                 float sound_speed_m_s, float sampling_freq_hz, float demod_freq_hz,
+                                                 float f_number);
+
+/* reference rcabeam.h:67-85: channel sums [v, c], angle sums [v, a], active counts [v]. */
+rcabeam_status rcabeam_delay_rca_channel_data_device(const void* iq_ch, const float* scan_coords_m,
+                                                     const float* elements_m, const float* angles_rad,
+                                                     const float* t_start_s, void* channel_sum, void* angle_sum,
+                                                     float* n_active, size_t n_samples, size_t n_channels,
+                                                     size_t n_angles, size_t n_voxels, int config,
+                                                     float sound_speed_m_s, float sampling_freq_hz,
+                                                     float demod_freq_hz, float f_number);
+
+/* reference rcabeam.h:87-104: |sum RC + CR|^2 of one frame. */
+rcabeam_status rcabeam_opw_pd_from_channels_device(const void* iq_rc, const void* iq_cr, const float* scan_coords_m,
+                                                   const float* x_elements_m, const float* y_elements_m,
+                                                   const float* angles_rad, const float* t_start_s, float* out,
+                                                   size_t n_samples, size_t n_channels, size_t n_angles,
+                                                   size_t n_voxels, float sound_speed_m_s, float sampling_freq_hz,
+                                                   float demod_freq_hz, float f_number);
+
+/* reference rcabeam.h:106-123: |RC conj(CR)| of one frame. */
+rcabeam_status rcabeam_xdoppler_pd_from_channels_device(const void* iq_rc, const void* iq_cr,
+                                                        const float* scan_coords_m, const float* x_elements_m,
+                                                        const float* y_elements_m, const float* angles_rad,
+                                                        const float* t_start_s, float* out, size_t n_samples,
+                                                        size_t n_channels, size_t n_angles, size_t n_voxels,
+                                                        float sound_speed_m_s, float sampling_freq_hz,
+                                                        float demod_freq_hz, float f_number);
+
+/* reference rcabeam.h:125-142: |(sum_a sqrt RC_a)(sum_a sqrt CR_a)|^2 of one frame. */
+rcabeam_status rcabeam_rc_fmas_pd_from_channels_device(const void* iq_rc, const void* iq_cr,
+                                                       const float* scan_coords_m, const float* x_elements_m,
+                                                       const float* y_elements_m, const float* angles_rad,
+                                                       const float* t_start_s, float* out, size_t n_samples,
+                                                       size_t n_channels, size_t n_angles, size_t n_voxels,
+                                                       float sound_speed_m_s, float sampling_freq_hz,
+                                                       float demod_freq_hz, float f_number);
+
+/* reference rcabeam.h:144-163: OPW, XDoppler and RC-FMAS of one frame in one pass. */
+rcabeam_status rcabeam_fast_pd_from_channels_device(const void* iq_rc, const void* iq_cr, const float* scan_coords_m,
+                                                    const float* x_elements_m, const float* y_elements_m,
+                                                    const float* angles_rad, const float* t_start_s, float* opw_out,
+                                                    float* xdoppler_out, float* rc_fmas_out, size_t n_samples,
+                                                    size_t n_channels, size_t n_angles, size_t n_voxels,
+                                                    float sound_speed_m_s, float sampling_freq_hz,
+                                                    float demod_freq_hz, float f_number);
+
+/* reference rcabeam.h:165-182: DMAS * CCF * ACF of one frame. */
+rcabeam_status rcabeam_dmas_ccf_acf_from_channels_device(const void* iq_rc, const void* iq_cr,
+                                                         const float* scan_coords_m, const float* x_elements_m,
+                                                         const float* y_elements_m, const float* angles_rad,
+                                                         const float* t_start_s, float* out, size_t n_samples,
+                                                         size_t n_channels, size_t n_angles, size_t n_voxels,
+                                                         float sound_speed_m_s, float sampling_freq_hz,
+                                                         float demod_freq_hz, float f_number);
+
+/* ---- Frame-batched ensemble path (the OPW hot path). ------------------- */
+
+/* reference rcabeam.h:184-185: (samples, channels, angles, frames) complex64 ->
+ * (channels, angles, samples, frames) complex64.  Source and target must not alias. */
+rcabeam_status rcabeam_pack_ensemble_device(const void* source, void* target, size_t ns, size_t nc, size_t na,
+                                            size_t nt);
+
+/* reference rcabeam.h:187-207.  rc, cr: packed (channels, angles, samples, frames)
+ * complex64.  method: 0 OPW, 1 XDoppler, 2 RC-FMAS, 3 DMAS-CCF-ACF, 4 St-SW,
+ * 5 separate RC/CR IQ.  pd: 2*nv floats, the result is in the even entries.
+ * signal: optional complex64 (nv, nt) output ((nv, 2, nt) for method 5).
+ * weights/workspace: St-SW only.  geometry_workspace: caller-owned scratch of
+ * 2*nv*(nc+na) float4; this implementation computes delays on the fly and uses
+ * the scratch only for its voxel traversal order.  Delays and phases are formed
+ * in float64; interpolation and accumulation are float32. */
+rcabeam_status rcabeam_ensemble_device(const void* rc, const void* cr, const float* scan, const float* xe,
+                                       const float* ye, const float* angles, const float* starts, float* pd,
+                                       void* signal, float* weights, void* workspace, void* geometry_workspace,
+                                       size_t ns, size_t nc, size_t na, size_t nt, size_t nv, float c, float fs,
+                                       float fd, float fn, int method, int k);
+
+/* reference rcabeam.h:209-220: pack to complex FP16 (two IEEE halves, RN).
+ * range_error (one device int, zeroed by the caller) is set to 1 when a
+ * component is non-finite or beyond +/-65504. */
+rcabeam_status rcabeam_pack_ensemble_fp16_device(const void* source, void* target, int* range_error, size_t ns,
+                                                 size_t nc, size_t na, size_t nt);
+
+/* reference rcabeam.h:222-235: OPW from FP16-packed RC/CR; float32 geometry
+ * interpolation and accumulation, complex64 signal. */
+rcabeam_status rcabeam_opw_fp16_device(const void* rc, const void* cr, const float* scan, const float* xe,
+                                       const float* ye, const float* angles, const float* starts, float* pd,
+                                       void* signal, void* geometry_workspace, size_t ns, size_t nc, size_t na,
+                                       size_t nt, size_t nv, float c, float fs, float fd, float fn);
+
+/* ---- Extensions (no counterpart in the reference C interface). ---------- */
+
+/* Bytes of geometry_workspace that rcabeam_ensemble_device / rcabeam_opw_fp16_device
+ * actually use for nv voxels (at most the documented 2*nv*(nc+na) float4).  A
+ * buffer of this size may be passed instead of the documented one. */
+rcabeam_status rcabeam_ensemble_workspace_bytes(size_t nv, size_t nc, size_t na, size_t* bytes);
+
+/* Reads and clears the device error word set by a kernel whose bounded wait
+ * gave up (0 = no error).  Synchronizes the device. */
+rcabeam_status rcabeam_device_error(int* code);
+
+#ifdef __cplusplus
+}
+#endif

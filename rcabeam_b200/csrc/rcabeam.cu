@@ -1,0 +1,533 @@
+// rcabeam C ABI for B200 (sm_100a).  One translation unit: every kernel of the
+// library is included here so that the device error word is a single object.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cub/device/device_radix_sort.cuh>
+#include <mutex>
+
+#include "common.cuh"
+#include "das_generic.cuh"
+#include "das_staged.cuh"
+#include "pack.cuh"
+
+namespace rcb {
+
+// Device error word written by bounded waits that gave up.
+__device__ int g_device_error = 0;
+
+static int* device_error_ptr() {
+  int* p = nullptr;
+  if (cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_device_error) != cudaSuccess) return nullptr;
+  return p;
+}
+
+// ------------------------------------------------------------ TMA maps --
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// Packed (slabs = nc * na, ns, nt) ensemble as a 3-D tensor of elem_bytes elements.
+static bool make_slab_map(CUtensorMap* map, const void* base, int elem_bytes, size_t nt, size_t ns, size_t slabs,
+                          int box_frames, int box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {nt, ns, slabs};
+  cuuint64_t strides[2] = {nt * elem_bytes, nt * ns * elem_bytes};
+  cuuint32_t box[3] = {cuuint32_t(box_frames), cuuint32_t(box_rows), 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUtensorMapDataType dt = elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32;
+  return fn(map, dt, 3, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// -------------------------------------------------- voxel traversal order --
+// Morton (Z-order) codes of isotropically quantized voxel positions, sorted
+// with a radix sort, give tiles of 64 consecutive voxels that are compact in
+// space -- which keeps each tile's sample window short.  Uses the caller's
+// geometry workspace as scratch; returns nullptr (identity order) when the
+// call is small or the scratch does not fit.
+__device__ __forceinline__ unsigned ordered_bits(float f) {
+  unsigned u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float from_ordered(unsigned u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+__global__ void bbox_kernel(const float* scan, size_t nv, unsigned* box) {
+  unsigned lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, hi[3] = {0u, 0u, 0u};
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
+    for (int d = 0; d < 3; ++d) {
+      unsigned u = ordered_bits(scan[3 * i + d]);
+      lo[d] = min(lo[d], u);
+      hi[d] = max(hi[d], u);
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    for (int off = 16; off > 0; off >>= 1) {
+      lo[d] = min(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], off));
+      hi[d] = max(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], off));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(box + d, lo[d]);
+      atomicMax(box + 3 + d, hi[d]);
+    }
+  }
+}
+
+__device__ __forceinline__ unsigned spread10(unsigned x) {
+  x &= 0x3ffu;
+  x = (x | (x << 16)) & 0x030000ffu;
+  x = (x | (x << 8)) & 0x0300f00fu;
+  x = (x | (x << 4)) & 0x030c30c3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+
+__global__ void morton_kernel(const float* scan, size_t nv, const unsigned* box, unsigned* keys, unsigned* vals) {
+  size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  float lo[3], extent = 0.f;
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = from_ordered(box[d]);
+    extent = fmaxf(extent, from_ordered(box[3 + d]) - lo[d]);
+  }
+  float scale = extent > 0.f ? 1023.f / extent : 0.f;
+  unsigned q[3];
+  for (int d = 0; d < 3; ++d) {
+    float t = (scan[3 * i + d] - lo[d]) * scale + 0.5f;
+    q[d] = unsigned(fminf(fmaxf(t, 0.f), 1023.f));
+  }
+  // z (depth) is the slowest-varying bit of each triple so that lateral
+  // neighbours group first; depth moves the delay fastest.
+  keys[i] = (spread10(q[1]) << 2) | (spread10(q[0]) << 1) | spread10(q[2]);
+  vals[i] = unsigned(i);
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Scratch bytes of voxel_order for nv voxels (0 when no order is built).
+static size_t order_bytes(size_t nv, size_t* temp_bytes) {
+  if (nv < 2 * das::kTileVoxels || nv > 0x7fffffffull) return 0;
+  cub::DoubleBuffer<unsigned> keys(nullptr, nullptr), vals(nullptr, nullptr);
+  size_t temp = 0;
+  if (cub::DeviceRadixSort::SortPairs(nullptr, temp, keys, vals, int(nv), 0, 30, cudaStream_t(0)) != cudaSuccess)
+    return 0;
+  if (temp_bytes) *temp_bytes = temp;
+  return 4 * align256(nv * 4) + 256 + align256(temp);
+}
+
+static const unsigned* voxel_order(const float* scan, size_t nv, void* workspace, size_t workspace_bytes) {
+  size_t temp = 0;
+  size_t need = order_bytes(nv, &temp);
+  if (!need || need > workspace_bytes) return nullptr;
+  size_t n4 = align256(nv * 4);
+  cub::DoubleBuffer<unsigned> keys(nullptr, nullptr), vals(nullptr, nullptr);
+  unsigned char* w = static_cast<unsigned char*>(workspace);
+  unsigned* ka = reinterpret_cast<unsigned*>(w);
+  unsigned* kb = reinterpret_cast<unsigned*>(w + n4);
+  unsigned* va = reinterpret_cast<unsigned*>(w + 2 * n4);
+  unsigned* vb = reinterpret_cast<unsigned*>(w + 3 * n4);
+  unsigned* box = reinterpret_cast<unsigned*>(w + 4 * n4);
+  void* tmp = w + 4 * n4 + 256;
+  // 0xff.. bytes for the three minima, zero bytes for the three maxima.
+  if (cudaMemsetAsync(box, 0xff, 12, 0) != cudaSuccess || cudaMemsetAsync(box + 3, 0, 12, 0) != cudaSuccess)
+    return nullptr;
+  bbox_kernel<<<148, 256>>>(scan, nv, box);
+  morton_kernel<<<unsigned((nv + 255) / 256), 256>>>(scan, nv, box, ka, va);
+  keys = cub::DoubleBuffer<unsigned>(ka, kb);
+  vals = cub::DoubleBuffer<unsigned>(va, vb);
+  if (cub::DeviceRadixSort::SortPairs(tmp, temp, keys, vals, int(nv), 0, 30, cudaStream_t(0)) != cudaSuccess)
+    return nullptr;
+  if (cudaGetLastError() != cudaSuccess) return nullptr;
+  return vals.Current();
+}
+
+// ---------------------------------------------------------- dispatch --
+static unsigned pow2_at_least(unsigned x) {
+  unsigned p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+template <int LPV, bool HALF, int MODE, bool TMA>
+static rcabeam_status launch_staged(const CUtensorMap& mr, const CUtensorMap& mq, const das::Args& a, dim3 grid) {
+  using S = das::Shape<LPV, HALF>;
+  auto kern = das::opw_staged<LPV, HALF, MODE, TMA>;
+  size_t smem = S::bytes(a.na);
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+    return RCABEAM_ERROR_CUDA;
+  kern<<<grid, das::kThreads, smem>>>(mr, mq, a);
+  return launch_status();
+}
+
+template <bool HALF, int MODE, bool TMA>
+static rcabeam_status launch_lpv(int lpv, const CUtensorMap& mr, const CUtensorMap& mq, const das::Args& a,
+                                 dim3 grid) {
+  switch (lpv) {
+    case 32: return launch_staged<32, HALF, MODE, TMA>(mr, mq, a, grid);
+    case 16: return launch_staged<16, HALF, MODE, TMA>(mr, mq, a, grid);
+    case 8: return launch_staged<8, HALF, MODE, TMA>(mr, mq, a, grid);
+    case 4: return launch_staged<4, HALF, MODE, TMA>(mr, mq, a, grid);
+    default: return launch_staged<2, HALF, MODE, TMA>(mr, mq, a, grid);
+  }
+}
+
+template <bool HALF, int MODE>
+static rcabeam_status run_staged(das::Args a, size_t ntiles) {
+  const int elem = HALF ? 4 : 8;
+  const size_t nt = size_t(a.nt);
+  const bool aligned = (nt * elem) % 16 == 0 && reinterpret_cast<uintptr_t>(a.rc) % 16 == 0 &&
+                       reinterpret_cast<uintptr_t>(a.cr) % 16 == 0 && encode_fn() != nullptr;
+  const int main_chunks = int(nt / 64);
+  const int tail = int(nt % 64);
+  struct Launch {
+    int lpv, frames, chunks, base;
+  } launches[2];
+  int count = 0;
+  if (main_chunks) launches[count++] = {32, 64, main_chunks, 0};
+  if (tail) {
+    int frames = int(pow2_at_least(unsigned(tail)));
+    if (frames < 4) frames = 4;
+    launches[count++] = {frames / 2, frames, 1, main_chunks * 64};
+  }
+  for (int i = 0; i < count; ++i) {
+    CUtensorMap mr{}, mq{};
+    bool tma = aligned && make_slab_map(&mr, a.rc, elem, nt, size_t(a.ns), size_t(a.nc) * a.na,
+                                        launches[i].frames, das::kRows) &&
+               make_slab_map(&mq, a.cr, elem, nt, size_t(a.ns), size_t(a.nc) * a.na, launches[i].frames, das::kRows);
+    das::Args b = a;
+    b.frame_base = launches[i].base;
+    dim3 grid(unsigned(ntiles), unsigned(launches[i].chunks));
+    rcabeam_status st = tma ? launch_lpv<HALF, MODE, true>(launches[i].lpv, mr, mq, b, grid)
+                            : launch_lpv<HALF, MODE, false>(launches[i].lpv, mr, mq, b, grid);
+    if (st != RCABEAM_SUCCESS) return st;
+  }
+  return RCABEAM_SUCCESS;
+}
+
+template <bool HALF>
+static rcabeam_status ensemble_impl(const void* rc, const void* cr, const float* scan, const float* xe,
+                                    const float* ye, const float* angles, const float* starts, float* pd,
+                                    void* signal, float* weights, void* workspace, void* geometry_workspace, size_t ns,
+                                    size_t nc, size_t na, size_t nt, size_t nv, float c, float fs, float fd, float fn,
+                                    int method, int k) {
+  // Argument contract of the reference (ensemble.cu:664-675).
+  if (!rc || !cr || !scan || !xe || !ye || !angles || !starts || !pd || ns < 2 || !nc || !na || !nt || !nv ||
+      c <= 0 || fs <= 0 || method < 0 || method > 5 || (method == 5 && !signal) || !std::isfinite(c) ||
+      !std::isfinite(fs) || !std::isfinite(fd) || !std::isfinite(fn))
+    return RCABEAM_ERROR_ARGUMENT;
+  if (HALF && method != 0) return RCABEAM_ERROR_ARGUMENT;
+  if (method == 4 && (!weights || !workspace || signal || k < 2 || k > 4 || na < size_t(k)))
+    return RCABEAM_ERROR_ARGUMENT;
+  if (!geometry_workspace) return RCABEAM_ERROR_ARGUMENT;
+  // Index ranges of the kernels (32-bit sample, channel, angle, frame and voxel ids).
+  if (ns > INT32_MAX || nc > INT32_MAX || na > INT32_MAX || nt > INT32_MAX || nv > INT32_MAX ||
+      nc * na > INT32_MAX || na > 4096)
+    return RCABEAM_ERROR_ARGUMENT;
+  // St-SW is outside this build's scope.
+  if (method == 4) return RCABEAM_ERROR_ARGUMENT;
+  if (cudaMemsetAsync(pd, 0, 2 * nv * sizeof(float), 0) != cudaSuccess) return RCABEAM_ERROR_CUDA;
+  das::Args a{};
+  a.rc = rc;
+  a.cr = cr;
+  a.scan = scan;
+  a.xe = xe;
+  a.ye = ye;
+  a.angles = angles;
+  a.starts = starts;
+  a.pd = pd;
+  a.signal = static_cast<float2*>(signal);
+  a.ns = int(ns);
+  a.nc = int(nc);
+  a.na = int(na);
+  a.nt = int(nt);
+  a.nv = int(nv);
+  a.c = double(c);
+  a.fs = double(fs);
+  a.fd = double(fd);
+  a.fn = double(fn);
+  a.err = device_error_ptr();
+  if (method == 2 || method == 3) {
+    dim3 grid(unsigned((nv + generic::kWarps - 1) / generic::kWarps),
+              unsigned((nt + 32 * generic::kRegFrames - 1) / (32 * generic::kRegFrames)));
+    if (method == 2)
+      generic::ensemble_nonlinear<2><<<grid, generic::kWarps * 32>>>(a);
+    else
+      generic::ensemble_nonlinear<3><<<grid, generic::kWarps * 32>>>(a);
+    return launch_status();
+  }
+  // The caller owns 2 * nv * (nc + na) float4 of scratch (reference rcabeam.h:196).
+  a.order = voxel_order(scan, nv, geometry_workspace, 2 * nv * (nc + na) * 16);
+  const size_t ntiles = (nv + das::kTileVoxels - 1) / das::kTileVoxels;
+  rcabeam_status st;
+  if (method == 0)
+    st = run_staged<HALF, das::kOpw>(a, ntiles);
+  else if (method == 5)
+    st = run_staged<false, das::kApertures>(a, ntiles);
+  else
+    st = run_staged<false, das::kXdoppler>(a, ntiles);
+  if (st != RCABEAM_SUCCESS) return st;
+  if (method == 1) {
+    das::finish_magnitude<<<unsigned((nv + 255) / 256), 256>>>(pd, nv);
+    return launch_status();
+  }
+  return RCABEAM_SUCCESS;
+}
+
+static generic::FrameArgs frame_args(const void* rc, const void* cr, const float* scan, const float* xe,
+                                     const float* ye, const float* angles, const float* starts, size_t ns, size_t nc,
+                                     size_t na, size_t nv, float c, float fs, float fd, float fn) {
+  generic::FrameArgs f{};
+  f.rc = static_cast<const float2*>(rc);
+  f.cr = static_cast<const float2*>(cr);
+  f.scan = scan;
+  f.xe = xe;
+  f.ye = ye;
+  f.angles = angles;
+  f.starts = starts;
+  f.ns = int(ns);
+  f.nc = int(nc);
+  f.na = int(na);
+  f.nv = nv;
+  f.c = c;
+  f.fs = fs;
+  f.fd = fd;
+  f.fn = fn;
+  return f;
+}
+
+static bool bad_frame_args(const void* iq, const float* scan, const float* el, const float* angles,
+                           const float* starts, const void* out, size_t ns, size_t nc, size_t na, size_t nv,
+                           int config) {
+  return !iq || !scan || !el || !angles || !starts || !out || ns < 2 || !nc || !na || !nv ||
+         (config != 0 && config != 1) || ns > INT32_MAX || nc > INT32_MAX || na > INT32_MAX;
+}
+
+static unsigned blocks_for(size_t n, unsigned threads) { return unsigned((n + threads - 1) / threads); }
+
+}  // namespace rcb
+
+using namespace rcb;
+
+extern "C" {
+
+const char* rcabeam_status_string(rcabeam_status status) {
+  switch (status) {
+    case RCABEAM_SUCCESS: return "success";
+    case RCABEAM_ERROR_CUDA: return "cuda error";
+    case RCABEAM_ERROR_ARGUMENT: return "invalid argument";
+  }
+  return "unknown error";
+}
+
+rcabeam_status rcabeam_ensemble_workspace_bytes(size_t nv, size_t nc, size_t na, size_t* bytes) {
+  if (!bytes || !nv || !nc || !na) return RCABEAM_ERROR_ARGUMENT;
+  size_t need = order_bytes(nv, nullptr);
+  size_t documented = 2 * nv * (nc + na) * 16;
+  *bytes = need ? (need < documented ? need : documented) : 256;
+  return RCABEAM_SUCCESS;
+}
+
+rcabeam_status rcabeam_device_error(int* code) {
+  if (!code) return RCABEAM_ERROR_ARGUMENT;
+  if (cudaDeviceSynchronize() != cudaSuccess) return RCABEAM_ERROR_CUDA;
+  int zero = 0;
+  if (cudaMemcpyFromSymbol(code, g_device_error, sizeof(int)) != cudaSuccess) return RCABEAM_ERROR_CUDA;
+  if (cudaMemcpyToSymbol(g_device_error, &zero, sizeof(int)) != cudaSuccess) return RCABEAM_ERROR_CUDA;
+  return RCABEAM_SUCCESS;
+}
+
+rcabeam_status rcabeam_pack_ensemble_device(const void* source, void* target, size_t ns, size_t nc, size_t na,
+                                            size_t nt) {
+  if (!source || !target || !ns || !nc || !na || !nt || ns > SIZE_MAX / nc / na / nt) return RCABEAM_ERROR_ARGUMENT;
+  return launch_pack<false>(source, target, nullptr, ns, nc, na, nt);
+}
+
+rcabeam_status rcabeam_pack_ensemble_fp16_device(const void* source, void* target, int* range_error, size_t ns,
+                                                 size_t nc, size_t na, size_t nt) {
+  if (!source || !target || !range_error || !ns || !nc || !na || !nt || ns > SIZE_MAX / nc / na / nt ||
+      reinterpret_cast<uintptr_t>(source) % alignof(float2) != 0 ||
+      reinterpret_cast<uintptr_t>(target) % alignof(__half2) != 0 ||
+      reinterpret_cast<uintptr_t>(range_error) % alignof(int) != 0)
+    return RCABEAM_ERROR_ARGUMENT;
+  return launch_pack<true>(source, target, range_error, ns, nc, na, nt);
+}
+
+rcabeam_status rcabeam_ensemble_device(const void* rc, const void* cr, const float* scan, const float* xe,
+                                       const float* ye, const float* angles, const float* starts, float* pd,
+                                       void* signal, float* weights, void* workspace, void* geometry_workspace,
+                                       size_t ns, size_t nc, size_t na, size_t nt, size_t nv, float c, float fs,
+                                       float fd, float fn, int method, int k) {
+  return ensemble_impl<false>(rc, cr, scan, xe, ye, angles, starts, pd, signal, weights, workspace,
+                              geometry_workspace, ns, nc, na, nt, nv, c, fs, fd, fn, method, k);
+}
+
+rcabeam_status rcabeam_opw_fp16_device(const void* rc, const void* cr, const float* scan, const float* xe,
+                                       const float* ye, const float* angles, const float* starts, float* pd,
+                                       void* signal, void* geometry_workspace, size_t ns, size_t nc, size_t na,
+                                       size_t nt, size_t nv, float c, float fs, float fd, float fn) {
+  if (reinterpret_cast<uintptr_t>(rc) % alignof(__half2) != 0 ||
+      reinterpret_cast<uintptr_t>(cr) % alignof(__half2) != 0)
+    return RCABEAM_ERROR_ARGUMENT;
+  return ensemble_impl<true>(rc, cr, scan, xe, ye, angles, starts, pd, signal, nullptr, nullptr, geometry_workspace,
+                             ns, nc, na, nt, nv, c, fs, fd, fn, 0, 2);
+}
+
+// ------------------------------------------------- single-frame API --
+rcabeam_status rcabeam_opw_device(const void* iq, void* out, size_t n_voxels, size_t n_angles, size_t n_frames) {
+  if (!iq || !out || !n_voxels || !n_angles || !n_frames) return RCABEAM_ERROR_ARGUMENT;
+  generic::angles_opw<<<blocks_for(n_voxels * n_frames, 256), 256>>>(static_cast<const float2*>(iq),
+                                                                      static_cast<float2*>(out), n_voxels, n_angles,
+                                                                      n_frames);
+  return launch_status();
+}
+
+static rcabeam_status angle_pd(const void* iq, float* out, size_t nv, size_t na, size_t nt, size_t rs, size_t rn,
+                               size_t cs, size_t cn, int fmas) {
+  if (!iq || !out || !nv || !na || !nt) return RCABEAM_ERROR_ARGUMENT;
+  if (rs + rn > na || cs + cn > na) return RCABEAM_ERROR_ARGUMENT;
+  generic::angles_pd<<<blocks_for(nv, 256), 256>>>(static_cast<const float2*>(iq), out, nv, na, nt, rs, rn, cs, cn,
+                                                   fmas);
+  return launch_status();
+}
+
+rcabeam_status rcabeam_xdoppler_pd_device(const void* iq, float* out, size_t n_voxels, size_t n_angles,
+                                          size_t n_frames, size_t rc_start, size_t rc_count, size_t cr_start,
+                                          size_t cr_count) {
+  return angle_pd(iq, out, n_voxels, n_angles, n_frames, rc_start, rc_count, cr_start, cr_count, 0);
+}
+
+rcabeam_status rcabeam_rc_fmas_pd_device(const void* iq, float* out, size_t n_voxels, size_t n_angles,
+                                         size_t n_frames, size_t rc_start, size_t rc_count, size_t cr_start,
+                                         size_t cr_count) {
+  return angle_pd(iq, out, n_voxels, n_angles, n_frames, rc_start, rc_count, cr_start, cr_count, 1);
+}
+
+rcabeam_status rcabeam_delay_rca_channels_device(const void* iq_ch, const float* scan_coords_m,
+                                                 const float* elements_m, const float* angles_rad,
+                                                 const float* t_start_s, void* out, size_t n_samples,
+                                                 size_t n_channels, size_t n_angles, size_t n_voxels, int config,
+                                                 float sound_speed_m_s, float sampling_freq_hz, float demod_freq_hz,
+                                                 float f_number) {
+  if (bad_frame_args(iq_ch, scan_coords_m, elements_m, angles_rad, t_start_s, out, n_samples, n_channels, n_angles,
+                     n_voxels, config))
+    return RCABEAM_ERROR_ARGUMENT;
+  auto f = frame_args(iq_ch, nullptr, scan_coords_m, elements_m, elements_m, angles_rad, t_start_s, n_samples,
+                      n_channels, n_angles, n_voxels, sound_speed_m_s, sampling_freq_hz, demod_freq_hz, f_number);
+  generic::frame_angle_sums<<<blocks_for(n_voxels * n_angles, 128), 128>>>(f, config, static_cast<float2*>(out));
+  return launch_status();
+}
+
+rcabeam_status rcabeam_delay_rca_channel_data_device(const void* iq_ch, const float* scan_coords_m,
+                                                     const float* elements_m, const float* angles_rad,
+                                                     const float* t_start_s, void* channel_sum, void* angle_sum,
+                                                     float* n_active, size_t n_samples, size_t n_channels,
+                                                     size_t n_angles, size_t n_voxels, int config,
+                                                     float sound_speed_m_s, float sampling_freq_hz,
+                                                     float demod_freq_hz, float f_number) {
+  if (bad_frame_args(iq_ch, scan_coords_m, elements_m, angles_rad, t_start_s, angle_sum, n_samples, n_channels,
+                     n_angles, n_voxels, config) ||
+      !channel_sum || !n_active)
+    return RCABEAM_ERROR_ARGUMENT;
+  auto f = frame_args(iq_ch, nullptr, scan_coords_m, elements_m, elements_m, angles_rad, t_start_s, n_samples,
+                      n_channels, n_angles, n_voxels, sound_speed_m_s, sampling_freq_hz, demod_freq_hz, f_number);
+  generic::frame_angle_sums<<<blocks_for(n_voxels * n_angles, 128), 128>>>(f, config,
+                                                                             static_cast<float2*>(angle_sum));
+  generic::frame_channel_sums<<<blocks_for(n_voxels * n_channels, 128), 128>>>(
+      f, config, static_cast<float2*>(channel_sum), n_active);
+  return launch_status();
+}
+
+static rcabeam_status frame_pd(const void* iq_rc, const void* iq_cr, const float* scan, const float* xe,
+                               const float* ye, const float* angles, const float* starts, int which, float* o_opw,
+                               float* o_xd, float* o_fmas, float* o_dmas, size_t ns, size_t nc, size_t na, size_t nv,
+                               float c, float fs, float fd, float fn) {
+  float* first = o_opw ? o_opw : (o_xd ? o_xd : (o_fmas ? o_fmas : o_dmas));
+  if (bad_frame_args(iq_rc, scan, xe, angles, starts, first, ns, nc, na, nv, 0) || !iq_cr || !ye)
+    return RCABEAM_ERROR_ARGUMENT;
+  auto f = frame_args(iq_rc, iq_cr, scan, xe, ye, angles, starts, ns, nc, na, nv, c, fs, fd, fn);
+  generic::frame_reduce<<<blocks_for(nv, 128), 128>>>(f, which, o_opw, o_xd, o_fmas, o_dmas);
+  return launch_status();
+}
+
+rcabeam_status rcabeam_opw_pd_from_channels_device(const void* iq_rc, const void* iq_cr, const float* scan_coords_m,
+                                                   const float* x_elements_m, const float* y_elements_m,
+                                                   const float* angles_rad, const float* t_start_s, float* out,
+                                                   size_t n_samples, size_t n_channels, size_t n_angles,
+                                                   size_t n_voxels, float sound_speed_m_s, float sampling_freq_hz,
+                                                   float demod_freq_hz, float f_number) {
+  if (!out) return RCABEAM_ERROR_ARGUMENT;
+  return frame_pd(iq_rc, iq_cr, scan_coords_m, x_elements_m, y_elements_m, angles_rad, t_start_s,
+                  generic::kFrameOpw, out, nullptr, nullptr, nullptr, n_samples, n_channels, n_angles, n_voxels,
+                  sound_speed_m_s, sampling_freq_hz, demod_freq_hz, f_number);
+}
+
+rcabeam_status rcabeam_xdoppler_pd_from_channels_device(const void* iq_rc, const void* iq_cr,
+                                                        const float* scan_coords_m, const float* x_elements_m,
+                                                        const float* y_elements_m, const float* angles_rad,
+                                                        const float* t_start_s, float* out, size_t n_samples,
+                                                        size_t n_channels, size_t n_angles, size_t n_voxels,
+                                                        float sound_speed_m_s, float sampling_freq_hz,
+                                                        float demod_freq_hz, float f_number) {
+  if (!out) return RCABEAM_ERROR_ARGUMENT;
+  return frame_pd(iq_rc, iq_cr, scan_coords_m, x_elements_m, y_elements_m, angles_rad, t_start_s, generic::kFrameXd,
+                  nullptr, out, nullptr, nullptr, n_samples, n_channels, n_angles, n_voxels, sound_speed_m_s,
+                  sampling_freq_hz, demod_freq_hz, f_number);
+}
+
+rcabeam_status rcabeam_rc_fmas_pd_from_channels_device(const void* iq_rc, const void* iq_cr,
+                                                       const float* scan_coords_m, const float* x_elements_m,
+                                                       const float* y_elements_m, const float* angles_rad,
+                                                       const float* t_start_s, float* out, size_t n_samples,
+                                                       size_t n_channels, size_t n_angles, size_t n_voxels,
+                                                       float sound_speed_m_s, float sampling_freq_hz,
+                                                       float demod_freq_hz, float f_number) {
+  if (!out) return RCABEAM_ERROR_ARGUMENT;
+  return frame_pd(iq_rc, iq_cr, scan_coords_m, x_elements_m, y_elements_m, angles_rad, t_start_s,
+                  generic::kFrameFmas, nullptr, nullptr, out, nullptr, n_samples, n_channels, n_angles, n_voxels,
+                  sound_speed_m_s, sampling_freq_hz, demod_freq_hz, f_number);
+}
+
+rcabeam_status rcabeam_fast_pd_from_channels_device(const void* iq_rc, const void* iq_cr, const float* scan_coords_m,
+                                                    const float* x_elements_m, const float* y_elements_m,
+                                                    const float* angles_rad, const float* t_start_s, float* opw_out,
+                                                    float* xdoppler_out, float* rc_fmas_out, size_t n_samples,
+                                                    size_t n_channels, size_t n_angles, size_t n_voxels,
+                                                    float sound_speed_m_s, float sampling_freq_hz,
+                                                    float demod_freq_hz, float f_number) {
+  if (!opw_out || !xdoppler_out || !rc_fmas_out) return RCABEAM_ERROR_ARGUMENT;
+  return frame_pd(iq_rc, iq_cr, scan_coords_m, x_elements_m, y_elements_m, angles_rad, t_start_s,
+                  generic::kFrameOpw | generic::kFrameXd | generic::kFrameFmas, opw_out, xdoppler_out, rc_fmas_out,
+                  nullptr, n_samples, n_channels, n_angles, n_voxels, sound_speed_m_s, sampling_freq_hz,
+                  demod_freq_hz, f_number);
+}
+
+rcabeam_status rcabeam_dmas_ccf_acf_from_channels_device(const void* iq_rc, const void* iq_cr,
+                                                         const float* scan_coords_m, const float* x_elements_m,
+                                                         const float* y_elements_m, const float* angles_rad,
+                                                         const float* t_start_s, float* out, size_t n_samples,
+                                                         size_t n_channels, size_t n_angles, size_t n_voxels,
+                                                         float sound_speed_m_s, float sampling_freq_hz,
+                                                         float demod_freq_hz, float f_number) {
+  if (!out) return RCABEAM_ERROR_ARGUMENT;
+  return frame_pd(iq_rc, iq_cr, scan_coords_m, x_elements_m, y_elements_m, angles_rad, t_start_s,
+                  generic::kFrameDmas, nullptr, nullptr, nullptr, out, n_samples, n_channels, n_angles, n_voxels,
+                  sound_speed_m_s, sampling_freq_hz, demod_freq_hz, f_number);
+}
+
+}  // extern "C"

@@ -1,0 +1,107 @@
+"""Pin the float64 oracle to the reference's own outputs (golden vectors) and known answers."""
+
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import clutter, das, methods
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def _grid_scan(x, z, y):
+    return np.stack(np.meshgrid(x, z, y, indexing="ij"), -1).reshape(-1, 3)
+
+
+@pytest.fixture(scope="module")
+def g():
+    return np.load(GOLDEN / "das.npz")
+
+
+@pytest.mark.parametrize("tag,fnumber", [("full", None), ("f1", 1.0)])
+@pytest.mark.parametrize("config", ["RC", "CR"])
+def test_das_matches_reference_small(g, tag, fnumber, config):
+    """Per-angle and per-channel sums agree with reference sim._delay_numpy (complex64 storage)."""
+    scan = _grid_scan(g["small_x"], g["small_z"], g["small_y"])
+    iq = g["small_rc"] if config == "RC" else g["small_cr"]
+    el = g["small_xe"] if config == "RC" else g["small_ye"]
+    args = (iq, scan, el, g["small_angles"], g["small_starts"], 1540.0, float(g["small_fs"]), float(g["small_fd"]),
+            fnumber, config)
+    per_angle = das.aperture_das(*args, per_angle=True)
+    ref = g[f"small_{tag}_{config}_per_angle"].reshape(per_angle.shape)
+    np.testing.assert_allclose(per_angle, ref, rtol=1e-6, atol=1e-6)
+    ch, ang, cnt = methods.aperture_terms(*args)
+    np.testing.assert_allclose(ch, g[f"small_{tag}_{config}_per_channel"].reshape(ch.shape), rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(ang, ref, rtol=1e-6, atol=1e-6)
+    np.testing.assert_array_equal(cnt, g[f"small_{tag}_{config}_count"].ravel())
+
+
+@pytest.mark.parametrize("config", ["RC", "CR"])
+def test_das_matches_reference_targets(g, config):
+    """15 MHz / 20 MS/s simulated targets, fnumber 1: relative L2 at the reference's complex64 floor."""
+    scan = _grid_scan(g["target_x"], g["target_z"], g["target_y"])
+    iq = g["target_rc"] if config == "RC" else g["target_cr"]
+    mine = das.aperture_das(iq, scan, g["target_el"], g["target_angles"], float(g["target_t0"]), 1540.0, 20e6, 15e6,
+                            1.0, config, per_angle=True)
+    ref = g[f"target_{config}_per_angle"].reshape(mine.shape)
+    assert np.linalg.norm(mine - ref) / np.linalg.norm(ref) < 1e-6
+
+
+def test_closed_receive_window_known_answer(g):
+    """Reference tests/test_iq_sampling.py:255-266: [1, 2.5, 3, 0]."""
+    zero = np.zeros(1)
+    scan = _grid_scan(zero, np.array([0, 1.5, 2, 2.25]), zero)
+    raw = np.arange(1, 4, dtype=np.complex64).reshape(3, 1, 1)
+    out = das.aperture_das(raw, scan, zero, zero, 0.0, 2.0, 1.0, 0.0, None, "RC").ravel()
+    np.testing.assert_array_equal(out, [1, 2.5, 3, 0])
+    np.testing.assert_array_equal(out, g["closed_window"])
+
+
+def test_voxel_order_known_answer():
+    order = np.load(GOLDEN / "order.npz")
+    for key in order.files:
+        shape = tuple(int(s) for s in key.split("_")[1].split("x"))
+        np.testing.assert_array_equal(das.opw_voxel_order(shape), order[key])
+    np.testing.assert_array_equal(das.opw_voxel_order((4, 3, 8))[:8], [0, 1, 2, 3, 24, 25, 26, 27])
+
+
+def test_dmas_oracle_matches_reference(g):
+    """DMAS-CCF-ACF from per-frame channel/angle sums (reference dmas.py:32-85)."""
+    ref = np.load(GOLDEN / "dmas.npz")["dmas_f1_power"].ravel()
+    scan = _grid_scan(g["small_x"], g["small_z"], g["small_y"])
+    mine = methods.dmas_ccf_acf_power(g["small_rc"], g["small_cr"], scan, g["small_xe"], g["small_ye"],
+                                      g["small_angles"], g["small_starts"], 1540.0, float(g["small_fs"]),
+                                      float(g["small_fd"]), 1.0)
+    np.testing.assert_allclose(mine, ref, rtol=1e-5, atol=1e-5)
+
+
+def test_clutter_oracle_matches_reference():
+    c = np.load(GOLDEN / "clutter.npz")
+    for method in ("svd", "gram"):
+        values, basis = clutter.temporal_basis(c["spectrum_matrix"].reshape(3, 6, 6), method=method)
+        np.testing.assert_allclose(values, c[f"spectrum_{method}_values"], rtol=1e-10)
+        np.testing.assert_allclose(values, c["spectrum_values"], rtol=2e-6)
+        np.testing.assert_allclose(basis.conj().T @ basis, np.eye(6), atol=2e-14)
+        out = clutter.svd_clutter_filter(c["spectrum_matrix"].reshape(3, 6, 6), rank_start=1, rank_stop=4,
+                                         method=method)
+        np.testing.assert_allclose(out, c[f"spectrum_{method}_filtered"], rtol=1e-9, atol=1e-12)
+        tissue = clutter.svd_clutter_filter(c["tissue_iq"], rank_start=3, method=method)
+        ref = c[f"tissue_{method}_filtered"]
+        assert np.linalg.norm(tissue - ref) / np.linalg.norm(ref) < 1e-6  # reference casts back to complex64
+
+
+def test_clutter_oracle_policy():
+    with pytest.raises(ValueError):
+        clutter.temporal_basis(np.zeros((2, 3)), method="svd")
+    with pytest.raises(ValueError):
+        clutter.rank_interval(4, 3, 2)
+    with np.errstate(over="ignore", invalid="ignore"), pytest.raises(np.linalg.LinAlgError, match="rescale"):
+        clutter.temporal_basis(np.full((2, 3), 1e200 + 1e200j), method="gram")
+
+
+def test_power_doppler_oracle():
+    x = np.array([[1 + 1j, 2, 0, 1j]])
+    np.testing.assert_allclose(das.power_doppler(x), [(2 + 4 + 0 + 1) / 4])
