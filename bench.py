@@ -45,6 +45,7 @@ RANK_START = 3
 
 
 def workload():
+    """Elements, angles and (x, z, y) grid of the workload (GRID_SHAPE may be reduced for profiling)."""
     el = (np.arange(NC) - (NC - 1) / 2) * PITCH
     angles = np.deg2rad(np.linspace(-10, 10, NA))
     half = (NC - 1) / 2 * PITCH
@@ -147,6 +148,7 @@ def run_b200(args, rank: int, world: int) -> dict | None:
         stop.record()
         torch.cuda.synchronize()
     elapsed = start.elapsed_time(stop) / 1e3
+    plan.check()
     das_ms = [plan.collect_das_ms(e) for e in das_ms]
     if world > 1:
         t = torch.tensor([elapsed], device=dev)
@@ -168,6 +170,7 @@ def run_b200(args, rank: int, world: int) -> dict | None:
         out = plan.run_host(host_rc, host_cr)
     e_stop.record()
     torch.cuda.synchronize()
+    plan.check()
     e2e = e_start.elapsed_time(e_stop) / 1e3 / e_steps
 
     if rank != 0:
@@ -277,7 +280,14 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-voxels", type=int, default=192, help="oracle voxels per core for the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=int, nargs=3, default=None, metavar=("NX", "NZ", "NY"),
+                    help="reduced grid for profiling runs (the reported workload is the default)")
     args = ap.parse_args()
+    if args.grid:
+        global GRID_SHAPE
+        GRID_SHAPE = tuple(args.grid)
+        CONFIG["grid"] = list(GRID_SHAPE)
+        CONFIG["workload"] += f" (REDUCED grid {GRID_SHAPE} for profiling)"
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

@@ -145,6 +145,41 @@ rcabeam_status rcabeam_opw_fp16_device(const void* rc, const void* cr, const flo
 
 /* ---- Extensions (no counterpart in the reference C interface). ---------- */
 
+/* Clutter filter (reference src/rcabeam/gpu_clutter.py, a CuPy module there).
+ * IQ is a row-major (rows, nt) Casorati matrix, complex64 (complex128 = 0) or
+ * complex128 (complex128 = 1).  Gram and basis matrices are complex128. */
+
+/* *scale (device double, zeroed by the caller) = max(|re|, |im|) over n values
+ * (gpu_clutter.py:141). */
+rcabeam_status rcabeam_clutter_scale_device(const void* iq, size_t n, int complex128, double* scale);
+
+/* Adds the upper-triangle tiles of (X / s)^H (X / s), s = *scale (1 if zero),
+ * into upper (device, row-major nt x nt complex128, zeroed by the caller).
+ * precision: 0 float64 CUDA cores, 1 float32 CUDA cores, 2 TF32 tensor cores,
+ * 3 3xBF16 tensor cores.  Call once per array to estimate one shared basis
+ * (gpu_clutter.py:144-160). */
+rcabeam_status rcabeam_gram_accumulate_device(const void* iq, size_t rows, size_t nt, int complex128,
+                                              const double* scale, int precision, double* upper);
+
+/* gram (device, column-major nt x nt complex128) = (G + G^H) / (2 total_rows)
+ * from the accumulated upper tiles (gpu_clutter.py:160-161). */
+rcabeam_status rcabeam_gram_finish_device(const double* upper, double* gram, size_t nt, size_t total_rows);
+
+/* Float64 Hermitian eigendecomposition of gram (cuSOLVER zheevd): ascending
+ * eigenvalues; gram is overwritten by the column eigenvectors.  workspace holds
+ * rcabeam_heevd_workspace_bytes bytes; *info (device int) is the solver status. */
+rcabeam_status rcabeam_heevd_workspace_bytes(size_t nt, size_t* bytes);
+rcabeam_status rcabeam_heevd_device(double* gram, double* eigenvalues, size_t nt, void* workspace,
+                                    size_t workspace_bytes, int* info);
+
+/* Per row x: coordinates y = x V on k column-major (nt x k) complex128 vectors.
+ * mode bit 0: residual x - y V^H (else the retained part y V^H); bit 1: write
+ * it to out (input dtype).  power (device double[rows], optional when writing)
+ * receives |residual|^2 / nt, or sum |y|^2 / nt without bit 0 (gpu_clutter.py:196-273).
+ * nt <= 512. */
+rcabeam_status rcabeam_project_device(const void* iq, void* out, double* power, size_t rows, size_t nt,
+                                      int complex128, const double* vectors, size_t k, int mode);
+
 /* Bytes of geometry_workspace that rcabeam_ensemble_device / rcabeam_opw_fp16_device
  * actually use for nv voxels (at most the documented 2*nv*(nc+na) float4).  A
  * buffer of this size may be passed instead of the documented one. */

@@ -33,6 +33,12 @@ SIGNATURES: dict[str, list] = {
     "rcabeam_ensemble_device": [P, P, P, P, P, P, P, P, P, P, P, P, Z, Z, Z, Z, Z, F, F, F, F, I, I],
     "rcabeam_pack_ensemble_fp16_device": [P, P, P, Z, Z, Z, Z],
     "rcabeam_opw_fp16_device": [P, P, P, P, P, P, P, P, P, P, Z, Z, Z, Z, Z, F, F, F, F],
+    "rcabeam_clutter_scale_device": [P, Z, I, P],
+    "rcabeam_gram_accumulate_device": [P, Z, Z, I, P, I, P],
+    "rcabeam_gram_finish_device": [P, P, Z, Z],
+    "rcabeam_heevd_workspace_bytes": [Z, ctypes.POINTER(c_size_t)],
+    "rcabeam_heevd_device": [P, P, Z, P, Z, P],
+    "rcabeam_project_device": [P, P, P, Z, Z, I, P, Z, I],
     "rcabeam_ensemble_workspace_bytes": [Z, Z, Z, ctypes.POINTER(c_size_t)],
     "rcabeam_device_error": [ctypes.POINTER(c_int)],
 }

@@ -1,0 +1,234 @@
+// Global temporal SVD clutter filter kernels (reference src/rcabeam/gpu_clutter.py).
+//
+//   * scale:  max |component| of the Casorati matrix (gpu_clutter.py:141);
+//   * gram:   G = (X / s)^H (X / s) / rows over the upper triangle of 64 x 64
+//             frame tiles, split over row slices; CUDA-core float64 (the
+//             reference default) or float32 accumulation (its complex64 mode);
+//   * finish: Hermitian symmetrization into a column-major complex128 matrix;
+//   * project: per row, coordinates y = x V on k temporal vectors, then either
+//             the retained power sum |y|^2 / T or the residual x - y V^H
+//             (written out and/or reduced to power), float64 throughout
+//             (gpu_clutter.py:196-273).
+// The tensor-core Gram forms live in gram_tc.cuh.
+#pragma once
+
+#include "common.cuh"
+
+namespace rcb {
+namespace clutter {
+
+constexpr int kGramTile = 64;     // frame columns per Gram tile
+constexpr int kGramRows = 16;     // rows staged per iteration
+constexpr int kGramThreads = 256; // 16 x 16 threads, 4 x 4 complex outputs each
+
+template <typename T>
+struct Cx;
+template <>
+struct Cx<float> {
+  using type = float2;
+};
+template <>
+struct Cx<double> {
+  using type = double2;
+};
+
+template <typename IN>
+__device__ __forceinline__ double2 load_c(const IN* p, size_t i) {
+  if constexpr (sizeof(IN) == 8) {
+    float2 v = reinterpret_cast<const float2*>(p)[i];
+    return make_double2(v.x, v.y);
+  } else {
+    return reinterpret_cast<const double2*>(p)[i];
+  }
+}
+
+// Max over |re| and |im| (non-negative doubles order like their bit patterns).
+template <typename IN>
+__global__ void max_abs_kernel(const IN* x, size_t n, unsigned long long* out) {
+  double m = 0.0;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    double2 v = load_c(x, i);
+    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+  }
+  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(m)));
+}
+
+// Partial Gram of one upper-triangle tile (bi <= bj) over a slice of rows.
+// Each thread owns a 4 x 4 block of complex outputs; rows are staged through
+// shared memory already scaled and converted to the accumulation type.
+template <typename ACC, typename IN>
+__global__ void __launch_bounds__(kGramThreads)
+    gram_simt(const IN* __restrict__ x, size_t rows, int nt, const double* __restrict__ scale,
+              int tiles_per_row_block, double* __restrict__ gram) {
+  using C = typename Cx<ACC>::type;
+  __shared__ C si[kGramRows][kGramTile];
+  __shared__ C sj[kGramRows][kGramTile];
+  // Map blockIdx.x to the (bi, bj) upper-triangle tile.
+  int t = blockIdx.x, bi = 0;
+  int nb = tiles_per_row_block;
+  while (t >= nb - bi) {
+    t -= nb - bi;
+    ++bi;
+  }
+  const int bj = bi + t;
+  const int ti = threadIdx.x / 16, tj = threadIdx.x % 16;
+  const size_t slices = gridDim.y;
+  const size_t per = (rows + slices - 1) / slices;
+  const size_t r0 = blockIdx.y * per, r1 = min(rows, r0 + per);
+  ACC acc_r[4][4] = {}, acc_i[4][4] = {};
+  const ACC s = ACC(*scale > 0.0 ? 1.0 / *scale : 1.0);
+  for (size_t base = r0; base < r1; base += kGramRows) {
+    for (int e = threadIdx.x; e < kGramRows * kGramTile; e += kGramThreads) {
+      int rr = e / kGramTile, cc = e % kGramTile;
+      size_t r = base + rr;
+      int ci = bi * kGramTile + cc, cj = bj * kGramTile + cc;
+      double2 vi = (r < r1 && ci < nt) ? load_c(x, r * nt + ci) : make_double2(0.0, 0.0);
+      double2 vj = (r < r1 && cj < nt) ? load_c(x, r * nt + cj) : make_double2(0.0, 0.0);
+      si[rr][cc] = C{ACC(vi.x) * s, ACC(vi.y) * s};
+      sj[rr][cc] = C{ACC(vj.x) * s, ACC(vj.y) * s};
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int rr = 0; rr < kGramRows; ++rr) {
+      C a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        a[u] = si[rr][ti + 16 * u];
+        b[u] = sj[rr][tj + 16 * u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          // conj(a) * b
+          acc_r[u][v] = fma(a[u].x, b[v].x, fma(a[u].y, b[v].y, acc_r[u][v]));
+          acc_i[u][v] = fma(a[u].x, b[v].y, fma(-a[u].y, b[v].x, acc_i[u][v]));
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      int i = bi * kGramTile + ti + 16 * u, j = bj * kGramTile + tj + 16 * v;
+      if (i < nt && j < nt) {
+        atomicAdd(gram + 2 * (size_t(i) * nt + j), double(acc_r[u][v]));
+        atomicAdd(gram + 2 * (size_t(i) * nt + j) + 1, double(acc_i[u][v]));
+      }
+    }
+  }
+}
+
+// Row-major upper-triangle partial sums -> column-major Hermitian complex128
+// matrix divided by rows: out = (G + G^H) / (2 rows) (gpu_clutter.py:161).
+__global__ void gram_finish(const double* upper, double* out, int nt, double inv_rows) {
+  int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nt) return;
+  int bi = i / kGramTile, bj = j / kGramTile;
+  // Entries of tiles below the diagonal were never accumulated: use conj(G[j][i]).
+  double2 gij = make_double2(0.0, 0.0), gji = make_double2(0.0, 0.0);
+  bool have_ij = bi <= bj, have_ji = bj <= bi;
+  if (have_ij) gij = make_double2(upper[2 * (size_t(i) * nt + j)], upper[2 * (size_t(i) * nt + j) + 1]);
+  if (have_ji) gji = make_double2(upper[2 * (size_t(j) * nt + i)], upper[2 * (size_t(j) * nt + i) + 1]);
+  if (!have_ij) gij = make_double2(gji.x, -gji.y);
+  if (!have_ji) gji = make_double2(gij.x, -gij.y);
+  double re = 0.5 * (gij.x + gji.x) * inv_rows;
+  double im = 0.5 * (gij.y - gji.y) * inv_rows;
+  // Column-major: element (i, j) at i + j * nt.
+  out[2 * (size_t(j) * nt + i)] = re;
+  out[2 * (size_t(j) * nt + i) + 1] = im;
+}
+
+constexpr int kProjChunk = 8;  // temporal vectors per register chunk
+
+// One warp per row.  vec: T x k complex128, column-major (vec[t + c * T]).
+// mode bit 0: subtract (residual x - (x V) V^H) else retained coordinates only;
+// bit 1: write filtered rows (same dtype as the input); power always written when non-null.
+template <typename IN, int MAXF>
+__global__ void __launch_bounds__(256)
+    project_rows(const IN* __restrict__ x, IN* __restrict__ out, double* __restrict__ power, size_t rows, int nt,
+                 const double2* __restrict__ vec, int k, int mode, double inv_nt) {
+  const int lane = threadIdx.x & 31;
+  const size_t row = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32;
+  if (row >= rows) return;
+  double2 xv[MAXF], proj[MAXF];
+#pragma unroll
+  for (int f = 0; f < MAXF; ++f) {
+    int t = lane + 32 * f;
+    xv[f] = t < nt ? load_c(x, row * nt + t) : make_double2(0.0, 0.0);
+    proj[f] = make_double2(0.0, 0.0);
+  }
+  double retained = 0.0;
+  for (int c0 = 0; c0 < k; c0 += kProjChunk) {
+    double2 y[kProjChunk];
+#pragma unroll
+    for (int c = 0; c < kProjChunk; ++c) {
+      double yr = 0.0, yi = 0.0;
+      if (c0 + c < k) {
+#pragma unroll
+        for (int f = 0; f < MAXF; ++f) {
+          int t = lane + 32 * f;
+          if (t < nt) {
+            double2 v = vec[t + size_t(c0 + c) * nt];
+            yr = fma(xv[f].x, v.x, fma(-xv[f].y, v.y, yr));
+            yi = fma(xv[f].x, v.y, fma(xv[f].y, v.x, yi));
+          }
+        }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        yr += __shfl_xor_sync(0xffffffffu, yr, off);
+        yi += __shfl_xor_sync(0xffffffffu, yi, off);
+      }
+      y[c] = make_double2(yr, yi);
+      retained += yr * yr + yi * yi;
+    }
+    if (mode & 3) {
+#pragma unroll
+      for (int f = 0; f < MAXF; ++f) {
+        int t = lane + 32 * f;
+        if (t < nt) {
+#pragma unroll
+          for (int c = 0; c < kProjChunk; ++c) {
+            if (c0 + c < k) {
+              // y * conj(v)
+              double2 v = vec[t + size_t(c0 + c) * nt];
+              proj[f].x = fma(y[c].x, v.x, fma(y[c].y, v.y, proj[f].x));
+              proj[f].y = fma(y[c].y, v.x, fma(-y[c].x, v.y, proj[f].y));
+            }
+          }
+        }
+      }
+    }
+  }
+  const bool subtract = mode & 1;
+  double pw = 0.0;
+#pragma unroll
+  for (int f = 0; f < MAXF; ++f) {
+    int t = lane + 32 * f;
+    if (t < nt) {
+      double2 r = subtract ? make_double2(xv[f].x - proj[f].x, xv[f].y - proj[f].y) : proj[f];
+      pw += r.x * r.x + r.y * r.y;
+      if (mode & 2) {
+        if constexpr (sizeof(IN) == 8)
+          reinterpret_cast<float2*>(out)[row * nt + t] = make_float2(float(r.x), float(r.y));
+        else
+          reinterpret_cast<double2*>(out)[row * nt + t] = r;
+      }
+    }
+  }
+  if (power) {
+    if (subtract) {
+      for (int off = 16; off > 0; off >>= 1) pw += __shfl_xor_sync(0xffffffffu, pw, off);
+      if (lane == 0) power[row] = pw * inv_nt;
+    } else if (lane == 0) {
+      power[row] = retained * inv_nt;
+    }
+  }
+}
+
+}  // namespace clutter
+}  // namespace rcb

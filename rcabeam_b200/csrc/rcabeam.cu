@@ -8,6 +8,9 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <mutex>
 
+#include <cusolverDn.h>
+
+#include "clutter.cuh"
 #include "common.cuh"
 #include "das_generic.cuh"
 #include "das_staged.cuh"
@@ -320,6 +323,39 @@ static bool bad_frame_args(const void* iq, const float* scan, const float* el, c
 
 static unsigned blocks_for(size_t n, unsigned threads) { return unsigned((n + threads - 1) / threads); }
 
+// One cuSOLVER handle per device, bound to the legacy default stream.
+static cusolverDnHandle_t solver_handle() {
+  static std::mutex lock;
+  static cusolverDnHandle_t handles[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> guard(lock);
+  if (!handles[dev]) {
+    if (cusolverDnCreate(&handles[dev]) != CUSOLVER_STATUS_SUCCESS) return nullptr;
+    cusolverDnSetStream(handles[dev], 0);
+  }
+  return handles[dev];
+}
+
+template <typename IN, int MAXF>
+static void launch_project(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
+                           size_t k, int mode) {
+  clutter::project_rows<IN, MAXF><<<blocks_for(rows * 32, 256), 256>>>(
+      static_cast<const IN*>(iq), static_cast<IN*>(out), power, rows, int(nt),
+      reinterpret_cast<const double2*>(vec), int(k), mode, 1.0 / double(nt));
+}
+
+template <typename IN>
+static void project_dispatch(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
+                             size_t k, int mode) {
+  size_t f = (nt + 31) / 32;
+  if (f <= 1) launch_project<IN, 1>(iq, out, power, rows, nt, vec, k, mode);
+  else if (f <= 2) launch_project<IN, 2>(iq, out, power, rows, nt, vec, k, mode);
+  else if (f <= 4) launch_project<IN, 4>(iq, out, power, rows, nt, vec, k, mode);
+  else if (f <= 8) launch_project<IN, 8>(iq, out, power, rows, nt, vec, k, mode);
+  else launch_project<IN, 16>(iq, out, power, rows, nt, vec, k, mode);
+}
+
 }  // namespace rcb
 
 using namespace rcb;
@@ -333,6 +369,91 @@ const char* rcabeam_status_string(rcabeam_status status) {
     case RCABEAM_ERROR_ARGUMENT: return "invalid argument";
   }
   return "unknown error";
+}
+
+// ------------------------------------------------ clutter-filter extensions --
+rcabeam_status rcabeam_clutter_scale_device(const void* iq, size_t n, int complex128, double* scale) {
+  if (!iq || !scale || !n) return RCABEAM_ERROR_ARGUMENT;
+  auto* out = reinterpret_cast<unsigned long long*>(scale);
+  if (complex128)
+    clutter::max_abs_kernel<double2><<<296, 256>>>(static_cast<const double2*>(iq), n, out);
+  else
+    clutter::max_abs_kernel<float2><<<296, 256>>>(static_cast<const float2*>(iq), n, out);
+  return launch_status();
+}
+
+rcabeam_status rcabeam_gram_accumulate_device(const void* iq, size_t rows, size_t nt, int complex128,
+                                              const double* scale, int precision, double* upper) {
+  if (!iq || !scale || !upper || !rows || !nt || nt > 65535) return RCABEAM_ERROR_ARGUMENT;
+  if (precision != 0 && precision != 1) return RCABEAM_ERROR_ARGUMENT;
+  int nb = int((nt + clutter::kGramTile - 1) / clutter::kGramTile);
+  unsigned tiles = unsigned(nb * (nb + 1) / 2);
+  size_t want = (148 * 8 + tiles - 1) / tiles;
+  size_t slices = (rows + clutter::kGramRows - 1) / clutter::kGramRows;
+  if (slices > want) slices = want;
+  if (slices > 65535) slices = 65535;
+  dim3 grid(tiles, unsigned(slices));
+  if (precision == 0) {
+    if (complex128)
+      clutter::gram_simt<double, double2><<<grid, clutter::kGramThreads>>>(static_cast<const double2*>(iq), rows,
+                                                                          int(nt), scale, nb, upper);
+    else
+      clutter::gram_simt<double, float2><<<grid, clutter::kGramThreads>>>(static_cast<const float2*>(iq), rows,
+                                                                         int(nt), scale, nb, upper);
+  } else {
+    if (complex128)
+      clutter::gram_simt<float, double2><<<grid, clutter::kGramThreads>>>(static_cast<const double2*>(iq), rows,
+                                                                         int(nt), scale, nb, upper);
+    else
+      clutter::gram_simt<float, float2><<<grid, clutter::kGramThreads>>>(static_cast<const float2*>(iq), rows,
+                                                                        int(nt), scale, nb, upper);
+  }
+  return launch_status();
+}
+
+rcabeam_status rcabeam_gram_finish_device(const double* upper, double* gram, size_t nt, size_t total_rows) {
+  if (!upper || !gram || !nt || !total_rows || nt > 65535) return RCABEAM_ERROR_ARGUMENT;
+  dim3 grid(blocks_for(nt, 128), unsigned(nt));
+  clutter::gram_finish<<<grid, 128>>>(upper, gram, int(nt), 1.0 / double(total_rows));
+  return launch_status();
+}
+
+rcabeam_status rcabeam_heevd_workspace_bytes(size_t nt, size_t* bytes) {
+  if (!bytes || !nt || nt > 65535) return RCABEAM_ERROR_ARGUMENT;
+  cusolverDnHandle_t h = solver_handle();
+  if (!h) return RCABEAM_ERROR_CUDA;
+  int lwork = 0;
+  if (cusolverDnZheevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, int(nt), nullptr, int(nt),
+                                  nullptr, &lwork) != CUSOLVER_STATUS_SUCCESS)
+    return RCABEAM_ERROR_CUDA;
+  *bytes = size_t(lwork) * sizeof(cuDoubleComplex);
+  return RCABEAM_SUCCESS;
+}
+
+rcabeam_status rcabeam_heevd_device(double* gram, double* eigenvalues, size_t nt, void* workspace,
+                                    size_t workspace_bytes, int* info) {
+  if (!gram || !eigenvalues || !workspace || !info || !nt || nt > 65535) return RCABEAM_ERROR_ARGUMENT;
+  cusolverDnHandle_t h = solver_handle();
+  if (!h) return RCABEAM_ERROR_CUDA;
+  if (cusolverDnSetStream(h, 0) != CUSOLVER_STATUS_SUCCESS) return RCABEAM_ERROR_CUDA;
+  int lwork = int(workspace_bytes / sizeof(cuDoubleComplex));
+  if (cusolverDnZheevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, int(nt),
+                       reinterpret_cast<cuDoubleComplex*>(gram), int(nt), eigenvalues,
+                       static_cast<cuDoubleComplex*>(workspace), lwork, info) != CUSOLVER_STATUS_SUCCESS)
+    return RCABEAM_ERROR_CUDA;
+  return launch_status();
+}
+
+rcabeam_status rcabeam_project_device(const void* iq, void* out, double* power, size_t rows, size_t nt,
+                                      int complex128, const double* vectors, size_t k, int mode) {
+  if (!iq || !rows || !nt || nt > 512 || (k && !vectors) || mode < 0 || mode > 3 || ((mode & 2) && !out) ||
+      (!power && !(mode & 2)))
+    return RCABEAM_ERROR_ARGUMENT;
+  if (complex128)
+    project_dispatch<double2>(iq, out, power, rows, nt, vectors, k, mode);
+  else
+    project_dispatch<float2>(iq, out, power, rows, nt, vectors, k, mode);
+  return launch_status();
 }
 
 rcabeam_status rcabeam_ensemble_workspace_bytes(size_t nv, size_t nc, size_t na, size_t* bytes) {

@@ -1,0 +1,148 @@
+"""End-to-end filtered OPW power Doppler on one GPU.
+
+``FilteredOpw`` is the resident form of the reference's filtered-OPW
+composition (examples/_support/clutter_pipeline.py:18-146): pack RC/CR ->
+OPW IQ (kept on the device) -> scaled temporal Gram -> float64 EVD ->
+clutter-filtered power Doppler.  All buffers are allocated once; ``run``
+launches every stage on the default stream without host synchronization
+except the final solver-status check, and records CUDA events per stage.
+``run_host`` adds the pinned host -> device upload of the channels and the
+device -> host read of the power, the boundary a host caller sees.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from rcabeam_b200 import _cuda_impl, _lib
+from rcabeam_b200.gpu_clutter import Gram
+from rcabeam_b200.sim import RCAGeometry, scan_coords
+
+_STAGES = ("pack", "das", "gram", "eig", "power")
+
+
+class FilteredOpw:
+    """Fixed-shape filtered-OPW pipeline: ``run(rc, cr) -> (nx, nz, ny)`` float64 filtered power."""
+
+    def __init__(self, channel_shape, angles, t_start, grid, geom: RCAGeometry, *, rank_start: int = 3,
+                 rank_stop: int | None = None, precision: str = "complex128", iq_storage: str = "float32"):
+        ns, nc, na, nt = (int(n) for n in channel_shape)
+        self.shape = (len(grid[0]), len(grid[1]), len(grid[2]))
+        self.channel_shape = (ns, nc, na, nt)
+        stop = nt if rank_stop is None else int(rank_stop)
+        if not 0 <= rank_start <= stop <= nt:
+            raise ValueError("Require 0 <= rank_start <= rank_stop <= number of frames")
+        self.rank = (int(rank_start), stop)
+        self.precision = precision
+        self.half = iq_storage == "float16"
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        scan = scan_coords(grid)
+        self.nv = len(scan)
+        f32 = lambda v: torch.from_numpy(np.array(v, dtype=np.float32)).to(dev)  # noqa: E731
+        self.scan = f32(scan)
+        self.xe, self.ye, self.angles = f32(geom.x_el), f32(geom.y_el), f32(angles)
+        self.starts = f32(np.broadcast_to(np.asarray(t_start, dtype=np.float32), (na,)))
+        self.consts = (float(geom.c), float(geom.fs), float(geom.f_demod),
+                       -1.0 if geom.fnumber is None else float(geom.fnumber))
+        elem = 4 if self.half else 8
+        self.packed = [torch.empty(ns * nc * na * nt * elem, dtype=torch.uint8, device=dev) for _ in range(2)]
+        self.range_error = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.geometry = torch.empty(_cuda_impl.workspace_bytes(self.nv, nc, na), dtype=torch.uint8, device=dev)
+        self.pd = torch.empty((self.nv, 2), dtype=torch.float32, device=dev)
+        self.iq = torch.empty((self.nv, nt), dtype=torch.complex64, device=dev)
+        self.gram = Gram(nt, dev)
+        self.power = torch.empty(self.nv, dtype=torch.float64, device=dev)
+        self.host_power = torch.empty(self.nv, dtype=torch.float64, pin_memory=True)
+        self.inputs = [torch.empty(self.channel_shape, dtype=torch.complex64, device=dev) for _ in range(2)]
+        start, stop = self.rank
+        self.subtract = stop - start > nt - (stop - start)
+        self.k = (start + nt - stop) if self.subtract else (stop - start)
+        self.vectors = torch.empty((max(self.k, 1), nt), dtype=torch.complex128, device=dev)
+        self.events = [torch.cuda.Event(enable_timing=True) for _ in range(len(_STAGES) + 1)]
+        self.last_das_event_ms = None
+
+    def _select_vectors(self) -> None:
+        """Column-major (T x k) vectors of the smaller projector from the ascending eigenvectors."""
+        nt = self.channel_shape[3]
+        start, stop = self.rank
+        vt = torch.view_as_complex(self.gram.matrix.view(nt, nt, 2))  # row e = e-th eigenvector (ascending)
+        desc = torch.arange(nt - 1, -1, -1, device=self.device)     # descending rank r -> eigenvector nt-1-r
+        ranks = torch.cat((desc[:start], desc[stop:])) if self.subtract else desc[start:stop]
+        if self.k:
+            torch.index_select(vt, 0, ranks, out=self.vectors[: self.k])
+
+    def run(self, rc: torch.Tensor, cr: torch.Tensor) -> torch.Tensor:
+        """Filtered power of resident complex64 RC/CR channels ``(ns, nc, na, nt)``."""
+        ns, nc, na, nt = self.channel_shape
+        ev = self.events
+        ev[0].record()
+        if self.half:
+            self.range_error.zero_()
+            for src, dst in zip((rc, cr), self.packed):
+                _lib.call("rcabeam_pack_ensemble_fp16_device", src.data_ptr(), dst.data_ptr(),
+                          self.range_error.data_ptr(), ns, nc, na, nt)
+        else:
+            for src, dst in zip((rc, cr), self.packed):
+                _lib.call("rcabeam_pack_ensemble_device", src.data_ptr(), dst.data_ptr(), ns, nc, na, nt)
+        ev[1].record()
+        _cuda_impl.opw_from_packed(self.packed[0], self.packed[1], self.scan, self.xe, self.ye, self.angles,
+                                   self.starts, self.pd, self.iq, self.geometry, ns, nc, na, nt, *self.consts,
+                                   self.half, synchronize=False)
+        ev[2].record()
+        self.gram.accumulate((self.iq,), self.precision)
+        ev[3].record()
+        self.gram.decompose()
+        ev[4].record()
+        if self.rank[0] == self.rank[1]:
+            self.power.zero_()
+        else:
+            self._select_vectors()
+            _lib.call("rcabeam_project_device", self.iq.data_ptr(), None, self.power.data_ptr(), self.nv, nt, 0,
+                      self.vectors.data_ptr(), self.k, 1 if self.subtract else 0)
+        ev[5].record()
+        self.last_das_event_ms = (ev[1], ev[2])
+        return self.power.view(self.shape)
+
+    def check(self) -> None:
+        """Synchronize and raise on solver or staging-pipeline failures."""
+        torch.cuda.synchronize()
+        if int(self.gram.info.item()):
+            raise np.linalg.LinAlgError("cuSOLVER eigendecomposition failed")
+        if self.half and int(self.range_error.item()):
+            raise ValueError("FP16 IQ requires finite components within +/-65504; rescale inputs explicitly")
+        if _lib.device_error():
+            raise _lib.RcabeamCudaError("a reconstruction kernel timed out waiting on its staging pipeline")
+
+    def run_host(self, rc_host: torch.Tensor, cr_host: torch.Tensor) -> torch.Tensor:
+        """Pinned host channels -> pinned host float64 filtered power (upload and download included)."""
+        self.inputs[0].copy_(rc_host, non_blocking=True)
+        self.inputs[1].copy_(cr_host, non_blocking=True)
+        self.run(self.inputs[0], self.inputs[1])
+        self.host_power.copy_(self.power, non_blocking=True)
+        return self.host_power
+
+    @staticmethod
+    def collect_das_ms(pair) -> float:
+        return pair[0].elapsed_time(pair[1])
+
+    def stage_ms(self) -> dict:
+        torch.cuda.synchronize()
+        return {name: round(self.events[i].elapsed_time(self.events[i + 1]), 3) for i, name in enumerate(_STAGES)}
+
+    @staticmethod
+    def launches_per_step() -> int:
+        # pack x2, voxel order (bbox, morton, 4 radix-sort passes), DAS main + tail,
+        # scale, Gram, finish, projection.
+        return 2 + 6 + 2 + 4
+
+
+def synthetic_channels(shape, *, generator: torch.Generator, device, scale: float = 1.0):
+    """Seeded complex Gaussian channel IQ ``(ns, nc, na, nt)`` for both apertures, made on the device."""
+    out = []
+    for _ in range(2):
+        re = torch.randn(shape, generator=generator, device=device, dtype=torch.float32)
+        im = torch.randn(shape, generator=generator, device=device, dtype=torch.float32)
+        out.append(torch.complex(re, im).mul_(scale))
+    return out

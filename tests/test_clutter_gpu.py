@@ -1,0 +1,212 @@
+"""GPU clutter filter and filtered-PD pipeline against the complex128 oracle (reference test_gpu_clutter.py)."""
+
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import clutter as oc
+from oracle import das
+from rcabeam_b200 import _lib, gpu_clutter, pipeline
+from rcabeam_b200.sim import RCAGeometry
+from tests._cases import oracle_inputs, rel_l2
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.fixture(autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("needs CUDA")
+    yield
+    assert _lib.device_error() == 0
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("shape", [(7,), (3, 7), (19, 6), (2, 4, 6), (2, 1), (16385, 4)])
+@pytest.mark.parametrize("dtype", [np.complex64, np.complex128])
+def test_gram_basis_and_filter_parity(shape, dtype):
+    rng = np.random.default_rng(8)
+    host = (rng.normal(size=shape) + 1j * rng.normal(size=shape)).astype(dtype)
+    iq = _dev(host)
+    original = iq.clone()
+    timings = {}
+    values, basis = gpu_clutter.temporal_basis(iq, timings=timings)
+    assert timings["matrix_seconds"] >= 0 and timings["decomposition_seconds"] >= 0
+    expected_values, _ = oc.temporal_basis(host)
+    np.testing.assert_allclose(values.cpu().numpy(), expected_values, rtol=1e-7, atol=1e-7)
+    np.testing.assert_allclose((basis.conj().T @ basis).cpu().numpy(), np.eye(shape[-1]), atol=2e-14)
+    end = min(3, shape[-1])
+    actual = gpu_clutter.apply_temporal_filter(iq, basis, rank_start=0, rank_stop=end)
+    expected = oc.svd_clutter_filter(host, rank_start=0, rank_stop=end)
+    assert actual.dtype == iq.dtype and tuple(actual.shape) == shape
+    assert torch.equal(iq, original)
+    np.testing.assert_allclose(actual.cpu().numpy(), expected, rtol=2e-6, atol=2e-6)
+    np.testing.assert_allclose(gpu_clutter.svd_clutter_filter(iq, rank_start=0).cpu().numpy(), host, atol=1e-6)
+    assert not gpu_clutter.apply_temporal_filter(iq, basis, rank_start=shape[-1]).cpu().numpy().any()
+
+
+def test_known_spectrum_golden():
+    c = np.load(GOLDEN / "clutter.npz")
+    iq = _dev(c["spectrum_matrix"].reshape(3, 6, 6))
+    values, basis = gpu_clutter.temporal_basis(iq)
+    np.testing.assert_allclose(values.cpu().numpy(), c["spectrum_values"], rtol=2e-6)
+    out = gpu_clutter.svd_clutter_filter(iq, rank_start=1, rank_stop=4)
+    np.testing.assert_allclose(out.cpu().numpy(), c["spectrum_gram_filtered"], rtol=2e-5, atol=2e-6)
+
+
+def test_tissue_clutter_rank3_golden():
+    """Strong rank-3 clutter removed: filtered IQ and power vs the reference (complex64 output)."""
+    c = np.load(GOLDEN / "clutter.npz")
+    iq = _dev(c["tissue_iq"])
+    out = gpu_clutter.svd_clutter_filter(iq, rank_start=3).cpu().numpy()
+    ref = c["tissue_gram_filtered"]
+    assert rel_l2(out, ref) < 1e-6
+    _, basis = gpu_clutter.temporal_basis(iq)
+    power = gpu_clutter.filtered_power(iq, basis, rank_start=3).cpu().numpy()
+    _, b64 = oc.temporal_basis(c["tissue_iq"], method="gram")
+    np.testing.assert_allclose(power, oc.filtered_power(c["tissue_iq"], b64, 3), rtol=1e-9)
+
+
+@pytest.mark.parametrize("start,stop,modes", [(2, 200, 2), (2, 5, 3), (0, 200, 0), (0, 0, 0), (200, 200, 0)])
+def test_smaller_projector_and_power(start, stop, modes):
+    rng = np.random.default_rng(12)
+    host = rng.normal(size=(17, 200)) + 1j * rng.normal(size=(17, 200))
+    iq = _dev(host)
+    basis = torch.eye(200, dtype=torch.complex128, device="cuda")
+    expected = np.zeros_like(host)
+    expected[:, start:stop] = host[:, start:stop]
+    actual = gpu_clutter.apply_temporal_filter(iq, basis, rank_start=start, rank_stop=stop)
+    power = gpu_clutter.filtered_power(iq, basis, rank_start=start, rank_stop=stop)
+    np.testing.assert_allclose(actual.cpu().numpy(), expected, atol=1e-13)
+    np.testing.assert_allclose(power.cpu().numpy(), np.mean(np.abs(expected) ** 2, axis=-1), atol=1e-13)
+    _, subtract = gpu_clutter._filter_vectors(basis, 200, start, stop)
+    assert subtract == (stop - start > 200 - (stop - start))
+
+
+def test_shared_rc_cr_basis_and_weak_band():
+    rng = np.random.default_rng(19)
+    left, _ = np.linalg.qr(rng.normal(size=(24, 6)) + 1j * rng.normal(size=(24, 6)))
+    right, _ = np.linalg.qr(rng.normal(size=(6, 6)) + 1j * rng.normal(size=(6, 6)))
+    host = (left * np.array([1e4, 2, 1, 0.3, 0.1, 0.01])) @ right.conj().T
+    pair = (_dev(host[:12].reshape(3, 4, 6)), _dev(host[12:].reshape(2, 6, 6)))
+    actual = gpu_clutter.svd_clutter_filter(pair, rank_start=1, rank_stop=5)
+    expected = oc.svd_clutter_filter(host, rank_start=1, rank_stop=5)
+    joined = np.concatenate([a.cpu().numpy().reshape(-1, 6) for a in actual])
+    assert rel_l2(joined, expected) < 1e-5
+
+
+@pytest.mark.parametrize("amplitude", [1e38, 1e-40])
+def test_scaled_gram_avoids_overflow_and_underflow(amplitude):
+    iq = torch.full((64, 8), complex(amplitude, amplitude), dtype=torch.complex64, device="cuda")
+    diagnostics = {}
+    values, basis = gpu_clutter.temporal_basis(iq, diagnostics=diagnostics)
+    expected, _ = oc.temporal_basis(iq.cpu().numpy())
+    assert values.dtype == torch.float64
+    np.testing.assert_allclose(float(values[0]), expected[0], rtol=2e-6)
+    assert diagnostics["input_scale"] == float(iq.real[0, 0])
+    power = gpu_clutter.filtered_power(iq, basis, rank_start=0)
+    np.testing.assert_allclose(power.cpu().numpy(), np.full(64, 2 * float(iq.real[0, 0]) ** 2), rtol=1e-6)
+
+
+def test_residual_power_does_not_subtract_large_energies():
+    basis = np.array([[1, 1, 1, 1], [1, -1, 1, -1], [1, 1, -1, -1], [1, -1, -1, 1]], complex).T / 2
+    host = (1e8 * basis[:, 0] + basis[:, 1])[None, :]
+    actual = gpu_clutter.filtered_power(_dev(host), _dev(basis), rank_start=1)
+    np.testing.assert_allclose(actual.cpu().numpy(), [0.25], atol=1e-14)
+
+
+def test_negative_eigenvalue_policy(monkeypatch):
+    decompose = gpu_clutter.Gram.decompose
+
+    def broken(self):
+        decompose(self)
+        self.eigenvalues[0] = -1.0
+
+    monkeypatch.setattr(gpu_clutter.Gram, "decompose", broken)
+    with pytest.raises(np.linalg.LinAlgError, match="negative"):
+        gpu_clutter.temporal_basis(torch.ones((3, 4), dtype=torch.complex128, device="cuda"))
+
+
+def test_invalid_inputs():
+    iq = torch.ones((3, 4), dtype=torch.complex64, device="cuda")
+    for bad in ((), np.ones((2, 4), complex), torch.ones((2, 4), device="cuda"),
+                torch.empty((0, 4), dtype=torch.complex64, device="cuda"),
+                torch.tensor([complex(np.nan, 1)], dtype=torch.complex64, device="cuda")):
+        with pytest.raises(ValueError):
+            gpu_clutter.temporal_basis(bad)
+    with pytest.raises(ValueError, match="frame count"):
+        gpu_clutter.temporal_basis((iq, torch.ones((3, 5), dtype=torch.complex64, device="cuda")))
+    with pytest.raises(ValueError, match="Precision"):
+        gpu_clutter.temporal_basis(iq, precision="float32")
+    for basis in (np.eye(4), torch.eye(3, dtype=torch.complex128, device="cuda"),
+                  torch.ones((4, 4), dtype=torch.complex128, device="cuda")):
+        with pytest.raises(ValueError, match="Basis"):
+            gpu_clutter.apply_temporal_filter(iq, basis, rank_start=0)
+    for start, stop in ((True, None), (-1, 4), (0, 5), (3, 2)):
+        with pytest.raises(ValueError, match=r"Rank|rank"):
+            gpu_clutter.svd_clutter_filter(iq, rank_start=start, rank_stop=stop)
+
+
+def test_power_doppler():
+    rng = np.random.default_rng(4)
+    x = (rng.normal(size=(5, 7, 33)) + 1j * rng.normal(size=(5, 7, 33))).astype(np.complex64)
+    np.testing.assert_allclose(gpu_clutter.power_doppler(x), das.power_doppler(x), rtol=1e-6)
+    np.testing.assert_allclose(gpu_clutter.power_doppler(_dev(x)).cpu().numpy(), das.power_doppler(x), rtol=1e-6)
+
+
+def _scene(frames=24, seed=5):
+    """Small RCA scene: slowly moving strong tissue speckle + weak random blood + noise."""
+    el = (np.arange(16) - 7.5) * 0.2e-3
+    geom = RCAGeometry(el, el, c=1540.0, fs=20e6, f_demod=15e6, fnumber=None)
+    angles = np.deg2rad(np.linspace(-8, 8, 3))
+    rng = np.random.default_rng(seed)
+    ns, t0 = 160, 4e-6
+    t = t0 + np.arange(ns) / 20e6
+    rc = np.zeros((ns, 16, 3, frames), np.complex128)
+    cr = np.zeros_like(rc)
+    pts = np.column_stack([rng.uniform(-1.5e-3, 1.5e-3, 60), rng.uniform(4e-3, 6e-3, 60),
+                           rng.uniform(-1.5e-3, 1.5e-3, 60)])
+    amp = rng.normal(size=60) + 1j * rng.normal(size=60)
+    amp[40:] *= 0.01
+    for f in range(frames):
+        shift = np.zeros(3)
+        shift[1] = 2e-6 * f
+        moved = pts + shift
+        moved[40:, 0] += 1e-5 * f * rng.normal()
+        for cfg, out in (("RC", rc), ("CR", cr)):
+            elx = el
+            for p, a in zip(moved, amp):
+                v, u = (p[0], p[2]) if cfg == "RC" else (p[2], p[0])
+                recv = np.sqrt(p[1] ** 2 + (v - elx) ** 2) / 1540.0
+                for m, th in enumerate(angles):
+                    tau = (p[1] * np.cos(th) + u * np.sin(th)) / 1540.0 + recv
+                    env = np.exp(-(((t[:, None] - tau[None, :]) / 0.15e-6) ** 2))
+                    out[:, :, m, f] += a * env * np.exp(-2j * np.pi * 15e6 * tau)[None, :]
+    noise = 1e-3 * (rng.normal(size=rc.shape) + 1j * rng.normal(size=rc.shape))
+    grid = (np.linspace(-1e-3, 1e-3, 6), np.linspace(4.2e-3, 5.8e-3, 10), np.linspace(-1e-3, 1e-3, 5))
+    return (rc + noise).astype(np.complex64), (cr + noise).astype(np.complex64), angles, t0, grid, geom
+
+
+def test_filtered_pipeline_matches_fp64_oracle():
+    """DAS -> Gram -> EVD -> filtered power vs the float64 oracle chain: relative L2 <= 1e-4 (target bar)."""
+    rc, cr, angles, t0, grid, geom = _scene()
+    o = oracle_inputs(angles, t0, grid, geom)
+    iq = das.opw_iq(rc, cr, o["scan"], o["xe"], o["ye"], o["angles"], o["starts"], o["c"], o["fs"], o["fd"],
+                    o["fnumber"])
+    _, basis = oc.temporal_basis(iq, method="gram")
+    expected = oc.filtered_power(iq, basis, 3).reshape(6, 10, 5)
+    plan = pipeline.FilteredOpw(rc.shape, angles, t0, grid, geom, rank_start=3)
+    got = plan.run(_dev(rc), _dev(cr))
+    plan.check()
+    assert rel_l2(got.cpu().numpy(), expected) < 1e-4
+    host = plan.run_host(torch.from_numpy(rc).pin_memory(), torch.from_numpy(cr).pin_memory())
+    plan.check()
+    assert rel_l2(host.numpy().reshape(6, 10, 5), expected) < 1e-4
