@@ -112,97 +112,144 @@ def peaks() -> dict:
 
 
 # ----------------------------------------------------------------- B200 arm --
-def run_b200(args, rank: int, world: int) -> dict | None:
+FORMS = {
+    # name: (packed IQ storage, Gram precision)
+    "chosen": ("bf16x2", "complex128"),
+    "plain": ("float32", "complex128"),
+    "fp16_storage": ("float16", "complex128"),
+}
+
+
+def _time_form(plan, rc, cr, steps: int, warmup: int, world: int, clocks=None):
+    """Device time of `steps` pipeline runs (max over ranks), after `warmup` runs."""
     import torch
 
-    from rcabeam_b200 import _lib, pipeline
-
-    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
-    torch.cuda.set_device(dev)
-    el, angles, grid = workload()
-    from rcabeam_b200.sim import RCAGeometry
-
-    geom = RCAGeometry(el, el, c=C, fs=FS, f_demod=FD, fnumber=None)
-    plan = pipeline.FilteredOpw((NS, NC, NA, NT), angles, T_START, grid, geom, rank_start=RANK_START)
-    gen = torch.Generator(device=dev).manual_seed(1234 + rank)
-    scene = pipeline.synthetic_channels((NS, NC, NA, NT), generator=gen, device=dev)
-    rc, cr = scene
-    torch.cuda.synchronize()
-
-    def step():
+    for _ in range(warmup):
         plan.run(rc, cr)
-
-    for _ in range(args.warmup):
-        step()
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    das_ms = []
-    with ClockSampler(dev.index) as clocks:
+    das = []
+    ctx = clocks if clocks is not None else _Null()
+    with ctx:
         torch.cuda.synchronize()
         start.record()
-        for _ in range(args.steps):
-            step()
-            das_ms.append(plan.last_das_event_ms)
+        for _ in range(steps):
+            plan.run(rc, cr)
+            das.append(plan.last_das_event_ms)
         stop.record()
         torch.cuda.synchronize()
-    elapsed = start.elapsed_time(stop) / 1e3
     plan.check()
-    das_ms = [plan.collect_das_ms(e) for e in das_ms]
+    elapsed = start.elapsed_time(stop) / 1e3
     if world > 1:
-        t = torch.tensor([elapsed], device=dev)
+        t = torch.tensor([elapsed], device=rc.device)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         elapsed = float(t.item())
-        torch.distributed.barrier()
+    das_s = statistics.median(plan.collect_das_ms(e) for e in das) / 1e3
+    return elapsed, das_s, plan.stage_ms()
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
+def run_b200(args, rank: int, world: int) -> dict | None:
+    import torch
+
+    from rcabeam_b200 import _lib, pipeline
+    from rcabeam_b200.sim import RCAGeometry
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    el, angles, grid = workload()
+    geom = RCAGeometry(el, el, c=C, fs=FS, f_demod=FD, fnumber=None)
+    gen = torch.Generator(device=dev).manual_seed(1234 + rank)
+    rc, cr = pipeline.synthetic_channels((NS, NC, NA, NT), generator=gen, device=dev)
+    torch.cuda.synchronize()
+    units = units_per_step()
+    results, powers = {}, {}
+    clock = None
+    for name in ("chosen", "plain", "fp16_storage"):
+        if name != "chosen" and args.only_chosen:
+            continue
+        storage, precision = FORMS[name]
+        plan = pipeline.FilteredOpw((NS, NC, NA, NT), angles, T_START, grid, geom, rank_start=RANK_START,
+                                    precision=precision, iq_storage=storage)
+        steps = args.steps if name == "chosen" else max(1, min(args.steps, 2))
+        warm = args.warmup if name == "chosen" else 1
+        sampler = ClockSampler(dev.index) if name == "chosen" else None
+        elapsed, das_s, stages = _time_form(plan, rc, cr, steps, warm, world, sampler)
+        if sampler is not None:
+            clock = sampler.summary()
+        powers[name] = plan.power.clone()
+        results[name] = {"ms_per_ensemble": round(elapsed / steps * 1e3, 3), "steps": steps,
+                         "gsamples_per_s": round(units * world * steps / elapsed / 1e9, 3),
+                         "das_ms": round(das_s * 1e3, 3), "stages_ms": stages, "iq_storage": storage,
+                         "gram_precision": precision}
+        if name == "chosen":
+            # End to end through the public pipeline: pinned host channels -> host filtered power.
+            host_rc, host_cr = rc.cpu().pin_memory(), cr.cpu().pin_memory()
+            plan.run_host(host_rc, host_cr)
+            torch.cuda.synchronize()
+            e_start, e_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e_steps = max(1, min(args.steps, 3))
+            e_start.record()
+            for _ in range(e_steps):
+                out = plan.run_host(host_rc, host_cr)
+            e_stop.record()
+            torch.cuda.synchronize()
+            plan.check()
+            e2e_s = e_start.elapsed_time(e_stop) / 1e3 / e_steps
+            e2e = {"value": round(units / e2e_s / 1e9, 3), "unit": "Gsamples/s",
+                   "ms_per_ensemble": round(e2e_s * 1e3, 3),
+                   "h2d_bytes_per_step": int(host_rc.numel() * 8 * 2),
+                   "d2h_bytes_per_step": int(out.numel() * out.element_size())}
+            launches = plan.launches_per_step()
+            del host_rc, host_cr
+        del plan
+        torch.cuda.empty_cache()
     assert _lib.device_error() == 0
-    clock = clocks.summary()
-
-    # End to end through the public API: pinned host channels -> host filtered power.
-    host_rc = rc.cpu().pin_memory()
-    host_cr = cr.cpu().pin_memory()
-    plan.run_host(host_rc, host_cr)
-    torch.cuda.synchronize()
-    e_start, e_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e_steps = max(1, min(args.steps, 3))
-    e_start.record()
-    for _ in range(e_steps):
-        out = plan.run_host(host_rc, host_cr)
-    e_stop.record()
-    torch.cuda.synchronize()
-    plan.check()
-    e2e = e_start.elapsed_time(e_stop) / 1e3 / e_steps
-
+    accuracy = {}
+    if "plain" in powers:
+        ref = powers["plain"]
+        for name in ("chosen", "fp16_storage"):
+            accuracy[f"{name}_vs_plain_filtered_pd_rel_l2"] = float(
+                torch.linalg.vector_norm(powers[name] - ref) / torch.linalg.vector_norm(ref))
     if rank != 0:
         return None
-    units = units_per_step()
-    value = units * world * args.steps / elapsed / 1e9
-    das_s = statistics.median(das_ms) / 1e3
+    ch = results["chosen"]
     pk = peaks()
-    # Compulsory DAS bytes per launch: packed channels read + IQ written + power written.
+    das_s = ch["das_ms"] / 1e3
+    # Tensor work of the dominant kernel: per (64-voxel tile, aperture, channel, angle)
+    # step, 3 MMAs of M=128 x N=2*frames x K=16 (sub-window splits excluded).
+    tiles = (int(np.prod(GRID_SHAPE)) + 63) // 64
+    mma_flops = tiles * 2 * NC * NA * 3 * 2 * 128 * (2 * ((NT + 7) // 8 * 8)) * 16
+    # Compulsory HBM bytes of one DAS launch: hi+lo packed planes read, IQ + power written.
     das_bytes = 2 * NS * NC * NA * NT * 8 + int(np.prod(GRID_SHAPE)) * NT * 8 + int(np.prod(GRID_SHAPE)) * 8
-    smem_peak = 148 * 128 * (clock["sm_mhz"] or 1965.0) * 1e6 / 1e9
+    tensor_peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops", 1590.0))
     line = {
-        "metric": "OPW Gsamples/s (vox*ch*ang*frm), filtered PD", "value": round(value, 3), "unit": "Gsamples/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(elapsed / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 (c64 IQ, f64 geometry, f64 Gram/eig/projection)",
-        "data": "synthetic seeded channel IQ (complex Gaussian speckle), full-size shapes", "config": CONFIG,
-        "filtered_pd_ms_per_ensemble": round(elapsed / args.steps * 1e3, 3),
-        "stages_ms": plan.stage_ms(),
-        "e2e": {"value": round(units / e2e / 1e9, 3), "unit": "Gsamples/s", "ms_per_ensemble": round(e2e * 1e3, 3),
-                "h2d_bytes_per_step": int(host_rc.numel() * 8 * 2),
-                "d2h_bytes_per_step": int(out.numel() * out.element_size())},
-        "roofline": {"bound": "hbm", "kernel": "opw_staged (DAS)", "achieved": round(das_bytes / das_s / 1e9, 2),
-                     "peak": pk.get("hbm_gbs"), "unit": "GB/s",
-                     "frac": round(das_bytes / das_s / 1e9 / pk.get("hbm_gbs", 6650.0), 5),
-                     "traffic": None, "das_ms": round(das_s * 1e3, 3),
-                     "note": "compulsory bytes; DAS is bound by shared-memory gathers, see gather_roofline"},
-        "gather_roofline": {"bound": "smem", "bytes_per_sample": 16, "achieved": round(units * 16 / das_s / 1e9, 1),
-                            "peak": round(smem_peak, 1), "unit": "GB/s",
-                            "frac": round(units * 16 / das_s / 1e9 / smem_peak, 4)},
+        "metric": "OPW Gsamples/s (vox*ch*ang*frm), filtered PD", "value": ch["gsamples_per_s"],
+        "unit": "Gsamples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ch["ms_per_ensemble"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 math on bf16x2-split c64 IQ (tcgen05 3-product DAS), f64 Gram/eig/projection",
+        "data": "synthetic seeded channel IQ (complex Gaussian), full-size shapes", "config": CONFIG,
+        "filtered_pd_ms_per_ensemble": {"chosen": ch["ms_per_ensemble"],
+                                         **({"plain": results["plain"]["ms_per_ensemble"]} if "plain" in results else {})},
+        "forms": results, "accuracy": accuracy, "e2e": e2e,
+        "roofline": {"bound": "tensor", "kernel": "opw_tc<bf16x3> (DAS)",
+                     "achieved": round(mma_flops / das_s / 1e12, 1), "peak": tensor_peak, "unit": "TFLOP/s",
+                     "frac": round(mma_flops / das_s / 1e12 / tensor_peak, 4), "traffic": None,
+                     "das_ms": ch["das_ms"],
+                     "note": "dense tcgen05 MMA flops issued per launch (3 x M128 x N400 x K16 per tile step) vs "
+                             "measured sustained bf16 peak (of measured); compulsory HBM bytes "
+                             f"{das_bytes / 1e9:.2f} GB per launch -> {das_bytes / das_s / 1e9:.1f} GB/s"},
         "clocks": clock,
-        "gpu_launches": plan.launches_per_step() * args.steps,
+        "gpu_launches": launches * args.steps,
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, reference_arm=False)
@@ -280,11 +327,22 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-voxels", type=int, default=192, help="oracle voxels per core for the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only-chosen", action="store_true", help="time only the chosen form (profiling runs)")
     ap.add_argument("--grid", type=int, nargs=3, default=None, metavar=("NX", "NZ", "NY"),
                     help="reduced grid for profiling runs (the reported workload is the default)")
+    ap.add_argument("--frames", type=int, default=None, help="reduced frame count for profiling runs")
+    ap.add_argument("--channels", type=int, default=None, help="reduced channel count for profiling runs")
     args = ap.parse_args()
+    global GRID_SHAPE, NT, NC
+    if args.channels:
+        NC = args.channels
+        CONFIG["channels"] = NC
+        CONFIG["workload"] += f" (REDUCED to {NC} channels for profiling)"
+    if args.frames:
+        NT = args.frames
+        CONFIG["frames"] = NT
+        CONFIG["workload"] += f" (REDUCED to {NT} frames for profiling)"
     if args.grid:
-        global GRID_SHAPE
         GRID_SHAPE = tuple(args.grid)
         CONFIG["grid"] = list(GRID_SHAPE)
         CONFIG["workload"] += f" (REDUCED grid {GRID_SHAPE} for profiling)"

@@ -145,6 +145,28 @@ rcabeam_status rcabeam_opw_fp16_device(const void* rc, const void* cr, const flo
 
 /* ---- Extensions (no counterpart in the reference C interface). ---------- */
 
+/* Packs complex64 (samples, channels, angles, frames) into two planes of
+ * (channels, angles, samples, frames) BF16 (re, im) pairs: hi = bf16(x) and
+ * lo = bf16(x - hi), the split operand of the three-product tensor-core OPW.
+ * range_error (one device int, zeroed by the caller) is set to 1 when a
+ * component is not finite.  Source must be 8-byte aligned; hi, lo 4-byte. */
+rcabeam_status rcabeam_pack_ensemble_split_device(const void* source, void* hi, void* lo, int* range_error, size_t ns,
+                                                  size_t nc, size_t na, size_t nt);
+
+/* OPW IQ and power on tcgen05 tensor cores (interpolation as a banded GEMM
+ * over 64-voxel tiles).  precision 0: rc_hi / cr_hi are FP16-packed channels
+ * (rcabeam_pack_ensemble_fp16_device), rc_lo / cr_lo unused; precision 1:
+ * BF16 hi / lo planes from rcabeam_pack_ensemble_split_device.  Coefficients
+ * are split into hi + lo halves; accumulation is float32.  pd, signal and
+ * geometry_workspace are as for rcabeam_ensemble_device (method 0).  Requires
+ * nt % 4 == 0 and 16-byte aligned planes (RCABEAM_ERROR_ARGUMENT otherwise).
+ * rcabeam_opw_fp16_device uses this kernel whenever its inputs qualify. */
+rcabeam_status rcabeam_opw_tc_device(const void* rc_hi, const void* rc_lo, const void* cr_hi, const void* cr_lo,
+                                     const float* scan, const float* xe, const float* ye, const float* angles,
+                                     const float* starts, float* pd, void* signal, void* geometry_workspace,
+                                     size_t ns, size_t nc, size_t na, size_t nt, size_t nv, float c, float fs,
+                                     float fd, float fn, int precision);
+
 /* Clutter filter (reference src/rcabeam/gpu_clutter.py, a CuPy module there).
  * IQ is a row-major (rows, nt) Casorati matrix, complex64 (complex128 = 0) or
  * complex128 (complex128 = 1).  Gram and basis matrices are complex128. */

@@ -54,17 +54,35 @@ def workspace_bytes(nv: int, nc: int, na: int) -> int:
     return int(out.value)
 
 
+def _storage(half_storage) -> str:
+    """Packed storage name: False/"float32", True/"float16", or "bf16x2"."""
+    if half_storage in (False, None, "float32"):
+        return "float32"
+    if half_storage in (True, "float16"):
+        return "float16"
+    if half_storage == "bf16x2":
+        return "bf16x2"
+    raise ValueError(f"unknown IQ storage {half_storage!r}")
+
+
 def ensemble_from_channels(rc, cr, scan, xe, ye, angles, starts, pd, signal, weights, c, fs, fd, fn, method, k,
                            half_storage) -> float:
-    """Upload, pack and reconstruct one ensemble; returns raw-upload wall seconds."""
+    """Upload, pack and reconstruct one ensemble; returns raw-upload wall seconds.
+
+    ``half_storage`` is the reference's FP16 flag; ``"bf16x2"`` selects the
+    split-BF16 tensor-core path (OPW only, frames a multiple of 4).
+    """
+    storage = _storage(half_storage)
     ns, nc, na, nt = rc.shape
     nv = scan.shape[0]
     if tuple(cr.shape) != tuple(rc.shape):
         raise ValueError("RC/CR ensemble shapes must match")
     if ns < 2 or not nc or not na or not nt or not nv or method < 0 or method > 5:
         raise ValueError("invalid ensemble dimensions or method")
-    if half_storage and method != 0:
+    if storage != "float32" and method != 0:
         raise ValueError("FP16 IQ storage is supported only for OPW")
+    if storage == "bf16x2" and nt % 4:
+        raise ValueError("bf16x2 storage requires a frame count divisible by 4")
     host_in = not isinstance(rc, torch.Tensor) or not rc.is_cuda
     begin = time.perf_counter()
     d_rc = _to_device(rc, torch.complex64)
@@ -85,32 +103,40 @@ def ensemble_from_channels(rc, cr, scan, xe, ye, angles, starts, pd, signal, wei
         d_sig = torch.empty((nv * planes, nt), dtype=torch.complex64, device=dev) if host_sig else signal
     else:
         d_sig = None
-    elem = 4 if half_storage else 8
+    elem = 8 if storage == "float32" else 4
     packed_rc = torch.empty(ns * nc * na * nt * elem, dtype=torch.uint8, device=dev)
     packed_cr = torch.empty_like(packed_rc)
-    if half_storage:
-        flag = torch.zeros(1, dtype=torch.int32, device=dev)
-        _lib.call("rcabeam_pack_ensemble_fp16_device", d_rc.data_ptr(), packed_rc.data_ptr(), flag.data_ptr(),
-                  ns, nc, na, nt)
-        _lib.call("rcabeam_pack_ensemble_fp16_device", d_cr.data_ptr(), packed_cr.data_ptr(), flag.data_ptr(),
-                  ns, nc, na, nt)
+    geometry = torch.empty(workspace_bytes(nv, nc, na), dtype=torch.uint8, device=dev)
+    flag = torch.zeros(1, dtype=torch.int32, device=dev)
+    if storage == "float16":
+        for src, dst in ((d_rc, packed_rc), (d_cr, packed_cr)):
+            _lib.call("rcabeam_pack_ensemble_fp16_device", src.data_ptr(), dst.data_ptr(), flag.data_ptr(),
+                      ns, nc, na, nt)
         if int(flag.item()):
             raise ValueError("FP16 IQ requires finite components within +/-65504; rescale inputs explicitly")
-    else:
-        _lib.call("rcabeam_pack_ensemble_device", d_rc.data_ptr(), packed_rc.data_ptr(), ns, nc, na, nt)
-        _lib.call("rcabeam_pack_ensemble_device", d_cr.data_ptr(), packed_cr.data_ptr(), ns, nc, na, nt)
-    geometry = torch.empty(workspace_bytes(nv, nc, na), dtype=torch.uint8, device=dev)
-    if half_storage:
         _lib.call("rcabeam_opw_fp16_device", packed_rc.data_ptr(), packed_cr.data_ptr(), d_scan.data_ptr(),
                   d_xe.data_ptr(), d_ye.data_ptr(), d_angles.data_ptr(), d_starts.data_ptr(), d_pd.data_ptr(),
                   _ptr(d_sig), geometry.data_ptr(), ns, nc, na, nt, nv, c, fs, fd, fn)
+    elif storage == "bf16x2":
+        lo_rc = torch.empty_like(packed_rc)
+        lo_cr = torch.empty_like(packed_rc)
+        for src, hi, lo in ((d_rc, packed_rc, lo_rc), (d_cr, packed_cr, lo_cr)):
+            _lib.call("rcabeam_pack_ensemble_split_device", src.data_ptr(), hi.data_ptr(), lo.data_ptr(),
+                      flag.data_ptr(), ns, nc, na, nt)
+        if int(flag.item()):
+            raise ValueError("bf16x2 IQ storage requires finite channel data")
+        _lib.call("rcabeam_opw_tc_device", packed_rc.data_ptr(), lo_rc.data_ptr(), packed_cr.data_ptr(),
+                  lo_cr.data_ptr(), d_scan.data_ptr(), d_xe.data_ptr(), d_ye.data_ptr(), d_angles.data_ptr(),
+                  d_starts.data_ptr(), d_pd.data_ptr(), _ptr(d_sig), geometry.data_ptr(), ns, nc, na, nt, nv, c, fs,
+                  fd, fn, 1)
     else:
-        w = None
         if method == 4:
             raise ValueError("St-SW is not provided by this implementation")
+        for src, dst in ((d_rc, packed_rc), (d_cr, packed_cr)):
+            _lib.call("rcabeam_pack_ensemble_device", src.data_ptr(), dst.data_ptr(), ns, nc, na, nt)
         _lib.call("rcabeam_ensemble_device", packed_rc.data_ptr(), packed_cr.data_ptr(), d_scan.data_ptr(),
                   d_xe.data_ptr(), d_ye.data_ptr(), d_angles.data_ptr(), d_starts.data_ptr(), d_pd.data_ptr(),
-                  _ptr(d_sig), w, None, geometry.data_ptr(), ns, nc, na, nt, nv, c, fs, fd, fn, method, k)
+                  _ptr(d_sig), None, None, geometry.data_ptr(), ns, nc, na, nt, nv, c, fs, fd, fn, method, k)
     torch.cuda.synchronize()
     if _lib.device_error():
         raise _lib.RcabeamCudaError("a reconstruction kernel timed out waiting on its staging pipeline")

@@ -33,6 +33,8 @@ SIGNATURES: dict[str, list] = {
     "rcabeam_ensemble_device": [P, P, P, P, P, P, P, P, P, P, P, P, Z, Z, Z, Z, Z, F, F, F, F, I, I],
     "rcabeam_pack_ensemble_fp16_device": [P, P, P, Z, Z, Z, Z],
     "rcabeam_opw_fp16_device": [P, P, P, P, P, P, P, P, P, P, Z, Z, Z, Z, Z, F, F, F, F],
+    "rcabeam_pack_ensemble_split_device": [P, P, P, P, Z, Z, Z, Z],
+    "rcabeam_opw_tc_device": [P, P, P, P, P, P, P, P, P, P, P, P, Z, Z, Z, Z, Z, F, F, F, F, I],
     "rcabeam_clutter_scale_device": [P, Z, I, P],
     "rcabeam_gram_accumulate_device": [P, Z, Z, I, P, I, P],
     "rcabeam_gram_finish_device": [P, P, Z, Z],

@@ -1,0 +1,516 @@
+// Tensor-core (tcgen05) RCA delay-and-sum: interpolation as a banded GEMM.
+//
+// For one (aperture, channel, angle) step and a tile of 64 spatially compact
+// voxels, every voxel's two interpolation taps fall in a window of <= 16
+// sample rows.  Writing the taps as a 128 x 16 coefficient matrix A -- row
+// 2v holds Re(phase * (1 - w), phase * w) of voxel v at its window rows,
+// row 2v + 1 the imaginary parts -- the step is
+//
+//     D[128, 2F] += A[128, 16] . X[16, 2F]
+//
+// where X is the staged window of packed channel samples with real and
+// imaginary parts interleaved along the frame axis (2F columns).  Lane 2v of
+// the TMEM accumulator then holds P = Re(A) X and lane 2v + 1 holds
+// Q = Im(A) X, and the voxel's IQ is (P_re - Q_im) + j (P_im + Q_re).
+// Accumulating all (aperture, channel, angle) steps in one TMEM accumulator
+// gives the OPW sum; the epilogue adds the power Doppler.
+//
+// Precision: FP16-packed channels are exact FP16; the coefficients are split
+// into FP16 hi + lo (two MMAs, ~22-bit coefficients).  Float32 channels are
+// pre-split into BF16 hi + lo planes; with BF16 hi/lo coefficients the step
+// uses three MMAs (Ahi Xhi + Alo Xhi + Ahi Xlo).  Accumulation is float32.
+//
+// Roles (224 threads, one CTA per SM, persistent over (tile, frame chunk)):
+//   warps 0-1   builders, one voxel per lane: per tile a table of float64
+//               transmit delays and transmit phases per (aperture, angle), per
+//               channel the float64 receive delay and phase; per step the tap
+//               (sample index, weight, phase by angle addition), the tile's
+//               row window (warp reductions + a named barrier), the A hi/lo
+//               rows (zero fill + two 16-bit stores), and lane 0 of warp 0
+//               issues the window's TMA boxes (64 columns x 16 rows, SWIZZLE_128B);
+//   warp 2      TMEM allocator; lane 0 issues tcgen05.mma and commits;
+//   warps 3-6   epilogue: tcgen05.ld of the accumulator, complex combine,
+//               IQ store and power.
+// Shared-memory operands: A is K-major without swizzle (8 x 16-byte core
+// matrices; LBO = 128 B between the two K cores, SBO = 256 B between 8-row
+// groups); X is MN-major SWIZZLE_128B straight from TMA (8-row x 128-byte
+// atoms; SBO = 1024 B between K groups, LBO = 2048 B between 64-column boxes).
+#pragma once
+
+#include <climits>
+
+#include "common.cuh"
+#include "das_staged.cuh"
+
+namespace rcb {
+namespace tc {
+
+constexpr int kVox = 64;
+constexpr int kRows = 16;
+constexpr int kStages = 4;
+constexpr int kBoxCols = 64;       // 16-bit columns per TMA box (one 128-byte swizzle atom)
+constexpr int kBoxBytes = kBoxCols * 2 * kRows;  // 2048
+constexpr int kMaxFrames = 256;    // frames per pass: 2 x frames float32 TMEM columns <= 512
+constexpr int kThreads = 224;
+constexpr int kBuilders = 2;  // builder warps (64 lanes = 64 voxels)
+constexpr int kTmemCols = 512;
+constexpr int kAMatBytes = 128 * kRows * 2;  // 4096: one 128 x 16 16-bit matrix
+// FP16 coefficients (|c| <= 1) are scaled by 2^10 before the hi/lo split so that
+// the lo halves of small coefficients stay out of the FP16 subnormal range; the
+// epilogue removes the power of two exactly.
+template <bool BF16X3>
+constexpr float kCoefScale = BF16X3 ? 1.0f : 1024.0f;
+enum Meta : int { kStep = 0, kTileEnd = 1, kFinish = 2 };
+
+struct Args {
+  const void* x_hi[2];  // per aperture (RC, CR): FP16 or BF16 hi planes, packed (c, a, s, 2 nt)
+  const void* x_lo[2];  // BF16 lo planes (three-product mode)
+  const float* scan;
+  const float* xe;
+  const float* ye;
+  const float* angles;
+  const float* starts;
+  const unsigned* order;
+  float* pd;
+  float2* signal;
+  int ns, nc, na, nt, nv;
+  double c, fs, fd, fn;
+  int frames;      // frames per pass (multiple of 8, <= 256)
+  int chunks;      // passes per tile
+  int ncols;       // 2 * frames
+  int nbox;        // TMA boxes per plane
+  int ntiles;
+  int* err;
+};
+
+template <bool BF16X3>
+struct Layout {
+  static constexpr int kPlanes = BF16X3 ? 2 : 1;
+  __host__ __device__ static size_t stage_bytes(int nbox) { return 2 * kAMatBytes + size_t(kPlanes) * nbox * kBoxBytes; }
+  // stages | control (barriers, meta, TMEM slot, window exchange) | angle table |
+  // per-tile transmit delays [2][na][64] double | transmit phases [2][na][64] float2
+  static size_t bytes(int nbox, int na) {
+    return kStages * stage_bytes(nbox) + 1024 + size_t(na) * 3 * sizeof(double) + size_t(na) * 2 * 64 * 16 + 1024;
+  }
+};
+
+// ------------------------------------------------------------- descriptors --
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo, uint32_t layout) {
+  uint64_t d = 0;
+  d |= uint64_t((addr >> 4) & 0x3fffu);
+  d |= uint64_t((lbo >> 4) & 0x3fffu) << 16;
+  d |= uint64_t((sbo >> 4) & 0x3fffu) << 32;
+  d |= uint64_t(1) << 46;  // descriptor version for sm_100
+  d |= uint64_t(layout & 7u) << 61;
+  return d;
+}
+constexpr uint32_t kLayoutNone = 0, kLayoutSw128 = 2;
+
+// kind::f16 instruction descriptor: F32 accumulate, A K-major, B MN-major.
+__host__ __device__ constexpr uint32_t instr_desc(bool bf16, int m, int n) {
+  return (1u << 4) | (uint32_t(bf16) << 7) | (uint32_t(bf16) << 10) | (0u << 15) | (1u << 16) |
+         (uint32_t(n >> 3) << 17) | (uint32_t(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 32 lanes x 32 consecutive 32-bit columns.
+__device__ __forceinline__ void tmem_ld32(uint32_t addr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// 16-bit split of a float: hi = round(x), lo = round(x - hi).
+template <bool BF16>
+__device__ __forceinline__ void split16(float x, unsigned short& hi, unsigned short& lo) {
+  if constexpr (BF16) {
+    __nv_bfloat16 h = __float2bfloat16_rn(x);
+    __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
+    hi = __bfloat16_as_ushort(h);
+    lo = __bfloat16_as_ushort(l);
+  } else {
+    __half h = __float2half_rn(x);
+    __half l = __float2half_rn(x - __half2float(h));
+    hi = __half_as_ushort(h);
+    lo = __half_as_ushort(l);
+  }
+}
+
+// Byte offset of element (row m, column k) of a K-major 128 x 16 no-swizzle operand.
+__device__ __forceinline__ uint32_t a_offset(int m, int k) {
+  return uint32_t((m >> 3) * 256 + (k >> 3) * 128 + (m & 7) * 16 + (k & 7) * 2);
+}
+
+// Zero one 16-element row of A hi and A lo, then store the two taps (r >= 0).
+template <bool BF16>
+__device__ __forceinline__ void put_row(unsigned char* a_hi, unsigned char* a_lo, int m, int r, float c0, float c1) {
+  const uint32_t o0 = a_offset(m, 0), o1 = a_offset(m, 8);
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  *reinterpret_cast<uint4*>(a_hi + o0) = zero;
+  *reinterpret_cast<uint4*>(a_hi + o1) = zero;
+  *reinterpret_cast<uint4*>(a_lo + o0) = zero;
+  *reinterpret_cast<uint4*>(a_lo + o1) = zero;
+  if (r >= 0) {
+    unsigned short h0, l0, h1, l1;
+    split16<BF16>(c0, h0, l0);
+    split16<BF16>(c1, h1, l1);
+    const uint32_t e0 = a_offset(m, r), e1 = a_offset(m, r + 1);
+    *reinterpret_cast<unsigned short*>(a_hi + e0) = h0;
+    *reinterpret_cast<unsigned short*>(a_lo + e0) = l0;
+    *reinterpret_cast<unsigned short*>(a_hi + e1) = h1;
+    *reinterpret_cast<unsigned short*>(a_lo + e1) = l1;
+  }
+}
+
+__device__ __forceinline__ void builders_sync() { asm volatile("bar.sync 1, %0;" ::"r"(kBuilders * 32) : "memory"); }
+
+// exp(+j 2 pi fd tau) with the cycle count reduced in float64.
+__device__ __forceinline__ float2 demod_phase(double fd, double tau) {
+  double cyc = fd * tau;
+  cyc -= rint(cyc);
+  float sn, cs;
+  sincospif(2.0f * float(cyc), &sn, &cs);
+  return make_float2(cs, sn);
+}
+
+template <bool BF16X3>
+__global__ void __launch_bounds__(kThreads, 1)
+    opw_tc(const __grid_constant__ CUtensorMap map_rc_hi, const __grid_constant__ CUtensorMap map_cr_hi,
+           const __grid_constant__ CUtensorMap map_rc_lo, const __grid_constant__ CUtensorMap map_cr_lo, Args p) {
+  using L = Layout<BF16X3>;
+  constexpr int kPlanes = L::kPlanes;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // Align the working area to 1024 bytes (SWIZZLE_128B atoms).
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const size_t stage_bytes = L::stage_bytes(p.nbox);
+  unsigned char* stages = smem;
+  unsigned char* ctrl = smem + kStages * stage_bytes;
+  uint64_t* full = reinterpret_cast<uint64_t*>(ctrl);
+  uint64_t* empty = full + kStages;
+  uint64_t* acc_full = empty + kStages;
+  uint64_t* acc_empty = acc_full + 1;
+  uint64_t* drain = acc_empty + 1;
+  int* meta = reinterpret_cast<int*>(drain + 1);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(meta + kStages);
+  int* xch = reinterpret_cast<int*>(ctrl + 512);  // [parity][builder warp][lo, hi]
+  double* angle_tab = reinterpret_cast<double*>(ctrl + 1024);
+  double* tx_delay = angle_tab + 3 * p.na;                                   // [2][na][64]
+  float2* tx_phase = reinterpret_cast<float2*>(tx_delay + 2 * p.na * kVox);  // [2][na][64]
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], kBuilders * 32);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, 4);
+    mbar_init(drain, 1);
+    fence_mbar_init();
+  }
+  for (int a = threadIdx.x; a < p.na; a += blockDim.x) {
+    double th = double(p.angles[a]);
+    angle_tab[3 * a] = cos(th);  // float64 transmit geometry per angle
+    angle_tab[3 * a + 1] = sin(th);
+    angle_tab[3 * a + 2] = double(p.starts[a]);
+  }
+  if (warp == kBuilders) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int work_items = p.ntiles * p.chunks;
+
+  if (warp < kBuilders) {
+    // ----------------------------------------------------------- builders --
+    const int v = 32 * warp + lane;  // voxel slot owned by this lane
+    const bool leader = warp == 0 && lane == 0;
+    if (leader) {
+      prefetch_tensormap(&map_rc_hi);
+      prefetch_tensormap(&map_cr_hi);
+      if constexpr (BF16X3) {
+        prefetch_tensormap(&map_rc_lo);
+        prefetch_tensormap(&map_cr_lo);
+      }
+    }
+    uint32_t k = 0, parity = 0;
+    bool ok = true;
+    const uint32_t tx_bytes = uint32_t(kPlanes * p.nbox * kBoxBytes);
+    const float sc = kCoefScale<BF16X3>;
+    // Waits for stage k to be free (uniform within a warp).  After a failed wait a
+    // builder stops waiting and writing but keeps executing the loops, so both
+    // builder warps always meet the same named barriers.
+    auto acquire = [&](int s) -> bool {
+      return __all_sync(0xffffffffu, mbar_wait(&empty[s], ((k / kStages) & 1) ^ 1, p.err, kErrWaitEmpty));
+    };
+    auto issue_tma = [&](unsigned char* stage, const CUtensorMap* mh, const CUtensorMap* ml, int col0, int row,
+                         int slab, int s) {
+      mbar_arrive_expect_tx(&full[s], tx_bytes);
+      unsigned char* b0 = stage + 2 * kAMatBytes;
+      for (int bx = 0; bx < p.nbox; ++bx) tma_load_3d(b0 + bx * kBoxBytes, mh, &full[s], col0 + bx * kBoxCols, row, slab);
+      if constexpr (BF16X3) {
+        unsigned char* b1 = b0 + p.nbox * kBoxBytes;
+        for (int bx = 0; bx < p.nbox; ++bx)
+          tma_load_3d(b1 + bx * kBoxBytes, ml, &full[s], col0 + bx * kBoxCols, row, slab);
+      }
+    };
+    for (int item = blockIdx.x; item < work_items; item += gridDim.x) {
+      const int tile = item / p.chunks, chunk = item % p.chunks;
+      const int col0 = 2 * chunk * p.frames;
+      int steps = 0;
+      const size_t qv = size_t(tile) * kVox + v;
+      const unsigned vid = qv < size_t(p.nv) ? (p.order ? p.order[qv] : unsigned(qv)) : UINT_MAX;
+      const bool valid = vid != UINT_MAX;
+      const size_t b3 = valid ? 3 * size_t(vid) : 0;
+      const double px = valid ? double(p.scan[b3]) : 0.0;
+      const double pz = valid ? double(p.scan[b3 + 1]) : 0.0;
+      const double py = valid ? double(p.scan[b3 + 2]) : 0.0;
+      // Per-tile transmit table (each lane reads back only its own entries).
+      for (int config = 0; config < 2; ++config) {
+        for (int a = 0; a < p.na; ++a) {
+          double ttx = transmit_delay(config ? px : py, pz, angle_tab[3 * a], angle_tab[3 * a + 1], p.c);
+          tx_delay[(config * p.na + a) * kVox + v] = ttx;
+          tx_phase[(config * p.na + a) * kVox + v] = demod_phase(p.fd, ttx);
+        }
+      }
+      for (int config = 0; config < 2; ++config) {
+        const float* el = config ? p.ye : p.xe;
+        const CUtensorMap* mh = config ? &map_cr_hi : &map_rc_hi;
+        const CUtensorMap* ml = config ? &map_cr_lo : &map_rc_lo;
+        for (int ch = 0; ch < p.nc; ++ch) {
+          bool act;
+          const double trx = receive_delay(config ? py : px, pz, double(el[ch]), p.c, p.fn, &act);
+          act = act && valid;
+          const float2 ph_rx = demod_phase(p.fd, trx);
+          for (int a = 0; a < p.na; ++a) {
+            const int ti = (config * p.na + a) * kVox + v;
+            const double tau = __dadd_rn(tx_delay[ti], trx);
+            const double sample = __dmul_rn(__dadd_rn(tau, -angle_tab[3 * a + 2]), p.fs);
+            const bool in_window = act && sample >= 0.0 && sample <= double(p.ns - 1);
+            const double fl = floor(sample);
+            const int i0 = in_window ? int(fl) : -1;
+            const float w = float(sample - fl);
+            // Window of the 64 voxels: warp reductions, exchanged between the two warps.
+            int lo = __reduce_min_sync(0xffffffffu, i0 >= 0 ? i0 : INT_MAX);
+            int hi = __reduce_max_sync(0xffffffffu, i0);
+            if (lane == 0) {
+              xch[(parity * kBuilders + warp) * 2] = lo;
+              xch[(parity * kBuilders + warp) * 2 + 1] = hi;
+            }
+            builders_sync();
+            lo = min(xch[parity * kBuilders * 2], xch[parity * kBuilders * 2 + 2]);
+            hi = max(xch[parity * kBuilders * 2 + 1], xch[parity * kBuilders * 2 + 3]);
+            parity ^= 1;
+            if (lo == INT_MAX) continue;  // no voxel of the tile sees this slab
+            const float2 pt = tx_phase[ti];
+            const float2 ph = make_float2(pt.x * ph_rx.x - pt.y * ph_rx.y, pt.x * ph_rx.y + pt.y * ph_rx.x);
+            // Coefficients of x[i0] and x[i0 + 1]: phase * (1 - w) and phase * w (scaled).
+            const float2 c0 = make_float2(sc * ph.x * (1.f - w), sc * ph.y * (1.f - w));
+            const float2 c1 = make_float2(sc * ph.x * w, sc * ph.y * w);
+            const int slab = ch * p.na + a;
+            for (int base = lo; base <= hi; base += kRows - 1) {
+              const int s = k % kStages;
+              if (ok) ok = acquire(s);
+              if (!ok) continue;  // failed: keep the barrier sequence, skip the work
+              unsigned char* stage = stages + size_t(s) * stage_bytes;
+              const int r = i0 - base;
+              const int rr = (i0 >= 0 && r >= 0 && r < kRows - 1) ? r : -1;
+              put_row<BF16X3>(stage, stage + kAMatBytes, 2 * v, rr, c0.x, c1.x);
+              put_row<BF16X3>(stage, stage + kAMatBytes, 2 * v + 1, rr, c0.y, c1.y);
+              if (leader) meta[s] = kStep;
+              fence_async_smem();
+              if (leader)
+                issue_tma(stage, mh, ml, col0, base, slab, s);
+              else
+                mbar_arrive(&full[s]);
+              ++k;
+              ++steps;
+            }
+          }
+        }
+      }
+      if (ok && steps == 0) {
+        // No voxel of the tile sees any sample: one all-zero step (zero
+        // coefficients; window beyond the last sample, which TMA fills with
+        // zeros) so that the accumulator is still initialized.
+        const int s = k % kStages;
+        if (ok) ok = acquire(s);
+        if (ok) {
+          unsigned char* stage = stages + size_t(s) * stage_bytes;
+          put_row<BF16X3>(stage, stage + kAMatBytes, 2 * v, -1, 0.f, 0.f);
+          put_row<BF16X3>(stage, stage + kAMatBytes, 2 * v + 1, -1, 0.f, 0.f);
+          if (leader) meta[s] = kStep;
+          fence_async_smem();
+          if (leader)
+            issue_tma(stage, &map_rc_hi, &map_rc_lo, col0, p.ns, 0, s);
+          else
+            mbar_arrive(&full[s]);
+          ++k;
+        }
+      }
+      // End of this work item.
+      if (ok) {
+        const int s = k % kStages;
+        if (ok) ok = acquire(s);
+        if (ok) {
+          if (leader) meta[s] = kTileEnd;
+          mbar_arrive(&full[s]);
+          ++k;
+        }
+      }
+      // The transmit table is rewritten for the next item only after both warps are done with it.
+      builders_sync();
+    }
+    if (ok) {
+      const int s = k % kStages;
+      if (ok) ok = acquire(s);
+      if (ok) {
+        if (leader) meta[s] = kFinish;
+        mbar_arrive(&full[s]);
+        ++k;
+      }
+    }
+    // Drain: every issued copy has landed before the builders leave.
+    for (uint32_t u = k > kStages ? k - kStages : 0; u < k; ++u)
+      mbar_wait(&full[u % kStages], (u / kStages) & 1, p.err, kErrWaitDrain);
+  } else if (warp == kBuilders) {
+    // ---------------------------------------------------------------- MMA --
+    if (lane == 0) {
+      const uint32_t n0 = p.ncols < 256 ? uint32_t(p.ncols) : 256u;
+      const uint32_t n1 = uint32_t(p.ncols) - n0;  // second part (0 if ncols <= 256)
+      const uint32_t id0 = instr_desc(BF16X3, 128, int(n0));
+      const uint32_t id1 = n1 ? instr_desc(BF16X3, 128, int(n1)) : 0u;
+      uint32_t k = 0, tiles_done = 0;
+      bool started = false;  // the current tile owns the accumulator
+      bool issued = false;   // the current tile has issued an MMA
+      bool ok = true;
+      for (;;) {
+        const int s = k % kStages;
+        if (!mbar_wait(&full[s], (k / kStages) & 1, p.err, kErrWaitFull)) {
+          ok = false;
+          break;
+        }
+        const int m = meta[s];
+        if (m == kFinish) break;
+        if (!started) {
+          // The previous tile's epilogue must have drained the accumulator.
+          if (tiles_done > 0 && !mbar_wait(acc_empty, (tiles_done - 1) & 1, p.err, kErrWaitEmpty)) {
+            ok = false;
+            break;
+          }
+          started = true;
+        }
+        tc_fence_after();
+        if (m == kTileEnd) {
+          mma_commit(acc_full);  // arrives once this tile's MMAs have completed
+          mbar_arrive(&empty[s]);
+          ++k;
+          ++tiles_done;
+          started = false;
+          issued = false;
+          continue;
+        }
+        const uint32_t st = smem_u32(stages + size_t(s) * stage_bytes);
+        const uint32_t a_hi = st, a_lo = st + kAMatBytes, b_hi = st + 2 * kAMatBytes;
+        const uint32_t b_lo = b_hi + uint32_t(p.nbox * kBoxBytes);
+        // Products: Ahi Xhi, Alo Xhi (+ Ahi Xlo for BF16 x3).
+        constexpr int kProducts = BF16X3 ? 3 : 2;
+#pragma unroll
+        for (int q = 0; q < kProducts; ++q) {
+          const uint32_t a = q == 1 ? a_lo : a_hi;
+          const uint32_t b = q == 2 ? b_lo : b_hi;
+          const uint64_t ad = smem_desc(a, 128, 256, kLayoutNone);
+          const uint32_t acc = (issued || q > 0) ? 1u : 0u;
+          mma_f16(tmem, ad, smem_desc(b, kBoxBytes, 1024, kLayoutSw128), id0, acc);
+          if (n1) mma_f16(tmem + 256, ad, smem_desc(b + 4 * kBoxBytes, kBoxBytes, 1024, kLayoutSw128), id1, acc);
+        }
+        issued = true;
+        mma_commit(&empty[s]);  // frees the stage once these MMAs have read it
+        ++k;
+      }
+      // Every issued MMA has completed before the warp leaves (TMEM is freed after).
+      mma_commit(drain);
+      mbar_wait(drain, 0, p.err, kErrWaitDrain);
+      (void)ok;
+    }
+    __syncwarp();
+  } else {
+    // ----------------------------------------------------------- epilogue --
+    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    const int m = 32 * q + lane;
+    const int v_slot = m >> 1;
+    const bool is_p = (m & 1) == 0;
+    uint32_t tiles_done = 0;
+    for (int item = blockIdx.x; item < work_items; item += gridDim.x) {
+      const int tile = item / p.chunks, chunk = item % p.chunks;
+      if (!__all_sync(0xffffffffu, mbar_wait(acc_full, tiles_done & 1, p.err, kErrWaitFull))) break;
+      tc_fence_after();
+      size_t qv = size_t(tile) * kVox + v_slot;
+      const unsigned v = qv < size_t(p.nv) ? (p.order ? p.order[qv] : unsigned(qv)) : UINT_MAX;
+      const int f0 = chunk * p.frames;
+      float power = 0.f;
+      for (int c0 = 0; c0 < p.ncols; c0 += 32) {
+        float val[32];
+        tmem_ld32(tmem + (uint32_t(32 * q) << 16) + uint32_t(c0), val);
+        // Partner lane holds the other half (P <-> Q) of the same voxel.
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          float other_re = __shfl_xor_sync(0xffffffffu, val[2 * i], 1);
+          float other_im = __shfl_xor_sync(0xffffffffu, val[2 * i + 1], 1);
+          // P lane: D = (P_re - Q_im, P_im + Q_re).
+          float dre = (val[2 * i] - other_im) * (1.0f / kCoefScale<BF16X3>);
+          float dim = (val[2 * i + 1] + other_re) * (1.0f / kCoefScale<BF16X3>);
+          int frame = f0 + (c0 >> 1) + i;
+          if (is_p && v != UINT_MAX && frame < p.nt && frame < f0 + p.frames) {
+            if (p.signal) p.signal[size_t(v) * p.nt + frame] = make_float2(dre, dim);
+            power += dre * dre + dim * dim;
+          }
+        }
+      }
+      if (is_p && v != UINT_MAX) atomicAdd(p.pd + 2 * size_t(v), power / float(p.nt));
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acc_empty);
+      ++tiles_done;
+    }
+  }
+  __syncthreads();
+  if (warp == kBuilders) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+}
+
+}  // namespace tc
+}  // namespace rcb

@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "das_generic.cuh"
 #include "das_staged.cuh"
+#include "das_tc.cuh"
 #include "pack.cuh"
 
 namespace rcb {
@@ -53,6 +54,20 @@ static bool make_slab_map(CUtensorMap* map, const void* base, int elem_bytes, si
   CUtensorMapDataType dt = elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32;
   return fn(map, dt, 3, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Packed 16-bit (re, im) plane (slabs, ns, 2 nt) as 16-bit elements with 64 x 16
+// SWIZZLE_128B boxes: the MN-major tensor-core operand layout.
+static bool make_plane_map(CUtensorMap* map, const void* base, size_t nt, size_t ns, size_t slabs) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {2 * nt, ns, slabs};
+  cuuint64_t strides[2] = {2 * nt * 2, 2 * nt * 2 * ns};
+  cuuint32_t box[3] = {cuuint32_t(tc::kBoxCols), cuuint32_t(tc::kRows), 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, const_cast<void*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -223,6 +238,49 @@ static rcabeam_status run_staged(das::Args a, size_t ntiles) {
   return RCABEAM_SUCCESS;
 }
 
+static bool tc_eligible(const void* const* planes, int count, size_t nt) {
+  if (nt % 4 != 0 || !encode_fn()) return false;
+  for (int i = 0; i < count; ++i)
+    if (!planes[i] || reinterpret_cast<uintptr_t>(planes[i]) % 16 != 0) return false;
+  return true;
+}
+
+// Tensor-core OPW over all (tile, frame chunk) work items with one persistent CTA per SM.
+template <bool BF16X3>
+static rcabeam_status run_tc(tc::Args a) {
+  const size_t nt = size_t(a.nt);
+  a.chunks = int((nt + tc::kMaxFrames - 1) / tc::kMaxFrames);
+  int frames = int((nt + a.chunks - 1) / a.chunks);
+  frames = (frames + 7) / 8 * 8;
+  a.frames = frames;
+  a.ncols = 2 * frames;
+  a.nbox = (a.ncols + tc::kBoxCols - 1) / tc::kBoxCols;
+  a.ntiles = int((size_t(a.nv) + tc::kVox - 1) / tc::kVox);
+  CUtensorMap mh[2], ml[2];
+  const size_t slabs = size_t(a.nc) * a.na;
+  for (int i = 0; i < 2; ++i) {
+    if (!make_plane_map(&mh[i], a.x_hi[i], nt, size_t(a.ns), slabs)) return RCABEAM_ERROR_CUDA;
+    if (BF16X3) {
+      if (!make_plane_map(&ml[i], a.x_lo[i], nt, size_t(a.ns), slabs)) return RCABEAM_ERROR_CUDA;
+    } else {
+      ml[i] = mh[i];
+    }
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  size_t smem = tc::Layout<BF16X3>::bytes(a.nbox, a.na) + 1024;
+  // Keep one CTA per SM: each CTA owns all 512 TMEM columns.
+  if (smem < 120 * 1024) smem = 120 * 1024;
+  auto kern = tc::opw_tc<BF16X3>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+    return RCABEAM_ERROR_CUDA;
+  const int items = a.ntiles * a.chunks;
+  const unsigned grid = unsigned(items < sms ? items : sms);
+  kern<<<grid, tc::kThreads, smem>>>(mh[0], mh[1], ml[0], ml[1], a);
+  return launch_status();
+}
+
 template <bool HALF>
 static rcabeam_status ensemble_impl(const void* rc, const void* cr, const float* scan, const float* xe,
                                     const float* ye, const float* angles, const float* starts, float* pd,
@@ -277,6 +335,31 @@ static rcabeam_status ensemble_impl(const void* rc, const void* cr, const float*
   // The caller owns 2 * nv * (nc + na) float4 of scratch (reference rcabeam.h:196).
   a.order = voxel_order(scan, nv, geometry_workspace, 2 * nv * (nc + na) * 16);
   const size_t ntiles = (nv + das::kTileVoxels - 1) / das::kTileVoxels;
+  const void* planes[2] = {rc, cr};
+  if (HALF && tc_eligible(planes, 2, nt) && nv <= size_t(INT32_MAX) - tc::kVox) {
+    tc::Args t{};
+    t.x_hi[0] = rc;
+    t.x_hi[1] = cr;
+    t.scan = scan;
+    t.xe = xe;
+    t.ye = ye;
+    t.angles = angles;
+    t.starts = starts;
+    t.order = a.order;
+    t.pd = pd;
+    t.signal = a.signal;
+    t.ns = a.ns;
+    t.nc = a.nc;
+    t.na = a.na;
+    t.nt = a.nt;
+    t.nv = a.nv;
+    t.c = a.c;
+    t.fs = a.fs;
+    t.fd = a.fd;
+    t.fn = a.fn;
+    t.err = a.err;
+    return run_tc<false>(t);
+  }
   rcabeam_status st;
   if (method == 0)
     st = run_staged<HALF, das::kOpw>(a, ntiles);
@@ -496,6 +579,61 @@ rcabeam_status rcabeam_ensemble_device(const void* rc, const void* cr, const flo
                                        float fd, float fn, int method, int k) {
   return ensemble_impl<false>(rc, cr, scan, xe, ye, angles, starts, pd, signal, weights, workspace,
                               geometry_workspace, ns, nc, na, nt, nv, c, fs, fd, fn, method, k);
+}
+
+rcabeam_status rcabeam_pack_ensemble_split_device(const void* source, void* hi, void* lo, int* range_error, size_t ns,
+                                                  size_t nc, size_t na, size_t nt) {
+  if (!source || !hi || !lo || !range_error || !ns || !nc || !na || !nt || ns > SIZE_MAX / nc / na / nt ||
+      reinterpret_cast<uintptr_t>(source) % alignof(float2) != 0 || reinterpret_cast<uintptr_t>(hi) % 4 != 0 ||
+      reinterpret_cast<uintptr_t>(lo) % 4 != 0 || reinterpret_cast<uintptr_t>(range_error) % alignof(int) != 0)
+    return RCABEAM_ERROR_ARGUMENT;
+  size_t rows = ns * nc * na;
+  size_t blocks = (rows + kPackThreads / 32 - 1) / (kPackThreads / 32);
+  if (blocks > 148ull * 64ull) blocks = 148ull * 64ull;
+  pack_split_rows<<<unsigned(blocks), kPackThreads>>>(static_cast<const float2*>(source),
+                                                      static_cast<__nv_bfloat162*>(hi),
+                                                      static_cast<__nv_bfloat162*>(lo), range_error, ns, nc, na, nt);
+  return launch_status();
+}
+
+rcabeam_status rcabeam_opw_tc_device(const void* rc_hi, const void* rc_lo, const void* cr_hi, const void* cr_lo,
+                                     const float* scan, const float* xe, const float* ye, const float* angles,
+                                     const float* starts, float* pd, void* signal, void* geometry_workspace,
+                                     size_t ns, size_t nc, size_t na, size_t nt, size_t nv, float c, float fs,
+                                     float fd, float fn, int precision) {
+  if (!rc_hi || !cr_hi || !scan || !xe || !ye || !angles || !starts || !pd || !geometry_workspace || ns < 2 ||
+      !nc || !na || !nt || !nv || c <= 0 || fs <= 0 || !std::isfinite(c) || !std::isfinite(fs) ||
+      !std::isfinite(fd) || !std::isfinite(fn) || (precision != 0 && precision != 1))
+    return RCABEAM_ERROR_ARGUMENT;
+  if (ns > INT32_MAX || nc * na > INT32_MAX || nt > INT32_MAX || nv > size_t(INT32_MAX) - tc::kVox || na > 4096)
+    return RCABEAM_ERROR_ARGUMENT;
+  const void* planes[4] = {rc_hi, cr_hi, rc_lo, cr_lo};
+  if (!tc_eligible(planes, precision == 1 ? 4 : 2, nt)) return RCABEAM_ERROR_ARGUMENT;
+  if (cudaMemsetAsync(pd, 0, 2 * nv * sizeof(float), 0) != cudaSuccess) return RCABEAM_ERROR_CUDA;
+  tc::Args t{};
+  t.x_hi[0] = rc_hi;
+  t.x_hi[1] = cr_hi;
+  t.x_lo[0] = rc_lo;
+  t.x_lo[1] = cr_lo;
+  t.scan = scan;
+  t.xe = xe;
+  t.ye = ye;
+  t.angles = angles;
+  t.starts = starts;
+  t.order = voxel_order(scan, nv, geometry_workspace, 2 * nv * (nc + na) * 16);
+  t.pd = pd;
+  t.signal = static_cast<float2*>(signal);
+  t.ns = int(ns);
+  t.nc = int(nc);
+  t.na = int(na);
+  t.nt = int(nt);
+  t.nv = int(nv);
+  t.c = c;
+  t.fs = fs;
+  t.fd = fd;
+  t.fn = fn;
+  t.err = device_error_ptr();
+  return precision == 1 ? run_tc<true>(t) : run_tc<false>(t);
 }
 
 rcabeam_status rcabeam_opw_fp16_device(const void* rc, const void* cr, const float* scan, const float* xe,

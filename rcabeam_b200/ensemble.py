@@ -16,7 +16,7 @@ from rcabeam_b200 import _cuda_impl
 from rcabeam_b200.sim import RCAGeometry, scan_coords
 
 Method = Literal["opw", "xdoppler", "rc_fmas", "dmas", "st_sw"]
-IQStorage = Literal["float32", "float16"]
+IQStorage = Literal["float32", "float16", "bf16x2"]
 _METHODS = {"opw": 0, "xdoppler": 1, "rc_fmas": 2, "dmas": 3, "st_sw": 4, "apertures": 5}
 
 
@@ -54,8 +54,8 @@ def _run(rc, cr, angles, t_start, grid, geom: RCAGeometry, method, k: int, retur
     """Validate ensemble inputs and execute the frame-batched CUDA path (reference ensemble.py:52-130)."""
     if method not in _METHODS or (method == "apertures" and not return_signal):
         raise ValueError(f"Unknown method: {method}")
-    if iq_storage not in ("float32", "float16") or (iq_storage == "float16" and method != "opw"):
-        raise ValueError("IQ storage must be float32, or float16 for OPW only")
+    if iq_storage not in ("float32", "float16", "bf16x2") or (iq_storage != "float32" and method != "opw"):
+        raise ValueError("IQ storage must be float32, or float16 / bf16x2 for OPW only")
     rc, cr = np.asarray(rc), np.asarray(cr)
     if rc.ndim != 4 or cr.shape != rc.shape or any(n == 0 for n in rc.shape) or rc.shape[0] < 2:
         raise ValueError("RC/CR must have matching nonempty (samples, channels, angles, frames) shapes")
@@ -95,7 +95,7 @@ def _run(rc, cr, angles, t_start, grid, geom: RCAGeometry, method, k: int, retur
         -1.0 if geom.fnumber is None else float(geom.fnumber),
         _METHODS[method],
         k,
-        iq_storage == "float16",
+        iq_storage,
     )
     if timings is not None:
         timings["raw_upload_seconds"] = raw_upload_seconds
@@ -113,7 +113,9 @@ def ensemble_pd_from_channels(rc, cr, angles, t_start, grid, geom: RCAGeometry, 
     OPW / RC-FMAS return the mean squared magnitude over frames, XDoppler the
     magnitude of the mean RC x conj(CR) product, DMAS the mean DMAS-CCF-ACF
     response.  ``iq_storage="float16"`` (OPW only) packs channels to FP16;
-    interpolation and accumulation stay float32.
+    interpolation and accumulation stay float32.  ``iq_storage="bf16x2"``
+    (OPW only, extension) packs float32 channels into BF16 hi/lo planes for the
+    three-product tensor-core path.
     """
     return _run(rc, cr, angles, t_start, grid, geom, method, k, False, timings, iq_storage)[0]
 

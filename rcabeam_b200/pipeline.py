@@ -35,6 +35,11 @@ class FilteredOpw:
             raise ValueError("Require 0 <= rank_start <= rank_stop <= number of frames")
         self.rank = (int(rank_start), stop)
         self.precision = precision
+        if iq_storage not in ("float32", "float16", "bf16x2"):
+            raise ValueError("IQ storage must be float32, float16 or bf16x2")
+        if iq_storage == "bf16x2" and nt % 4:
+            raise ValueError("bf16x2 storage requires a frame count divisible by 4")
+        self.storage = iq_storage
         self.half = iq_storage == "float16"
         dev = torch.device("cuda", torch.cuda.current_device())
         self.device = dev
@@ -46,8 +51,10 @@ class FilteredOpw:
         self.starts = f32(np.broadcast_to(np.asarray(t_start, dtype=np.float32), (na,)))
         self.consts = (float(geom.c), float(geom.fs), float(geom.f_demod),
                        -1.0 if geom.fnumber is None else float(geom.fnumber))
-        elem = 4 if self.half else 8
+        elem = 8 if iq_storage == "float32" else 4
         self.packed = [torch.empty(ns * nc * na * nt * elem, dtype=torch.uint8, device=dev) for _ in range(2)]
+        self.packed_lo = ([torch.empty(ns * nc * na * nt * elem, dtype=torch.uint8, device=dev) for _ in range(2)]
+                          if iq_storage == "bf16x2" else None)
         self.range_error = torch.zeros(1, dtype=torch.int32, device=dev)
         self.geometry = torch.empty(_cuda_impl.workspace_bytes(self.nv, nc, na), dtype=torch.uint8, device=dev)
         self.pd = torch.empty((self.nv, 2), dtype=torch.float32, device=dev)
@@ -78,18 +85,30 @@ class FilteredOpw:
         ns, nc, na, nt = self.channel_shape
         ev = self.events
         ev[0].record()
-        if self.half:
+        if self.storage == "float16":
             self.range_error.zero_()
             for src, dst in zip((rc, cr), self.packed):
                 _lib.call("rcabeam_pack_ensemble_fp16_device", src.data_ptr(), dst.data_ptr(),
+                          self.range_error.data_ptr(), ns, nc, na, nt)
+        elif self.storage == "bf16x2":
+            self.range_error.zero_()
+            for src, hi, lo in zip((rc, cr), self.packed, self.packed_lo):
+                _lib.call("rcabeam_pack_ensemble_split_device", src.data_ptr(), hi.data_ptr(), lo.data_ptr(),
                           self.range_error.data_ptr(), ns, nc, na, nt)
         else:
             for src, dst in zip((rc, cr), self.packed):
                 _lib.call("rcabeam_pack_ensemble_device", src.data_ptr(), dst.data_ptr(), ns, nc, na, nt)
         ev[1].record()
-        _cuda_impl.opw_from_packed(self.packed[0], self.packed[1], self.scan, self.xe, self.ye, self.angles,
-                                   self.starts, self.pd, self.iq, self.geometry, ns, nc, na, nt, *self.consts,
-                                   self.half, synchronize=False)
+        if self.storage == "bf16x2":
+            _lib.call("rcabeam_opw_tc_device", self.packed[0].data_ptr(), self.packed_lo[0].data_ptr(),
+                      self.packed[1].data_ptr(), self.packed_lo[1].data_ptr(), self.scan.data_ptr(),
+                      self.xe.data_ptr(), self.ye.data_ptr(), self.angles.data_ptr(), self.starts.data_ptr(),
+                      self.pd.data_ptr(), self.iq.data_ptr(), self.geometry.data_ptr(), ns, nc, na, nt, self.nv,
+                      *self.consts, 1)
+        else:
+            _cuda_impl.opw_from_packed(self.packed[0], self.packed[1], self.scan, self.xe, self.ye, self.angles,
+                                       self.starts, self.pd, self.iq, self.geometry, ns, nc, na, nt, *self.consts,
+                                       self.half, synchronize=False)
         ev[2].record()
         self.gram.accumulate((self.iq,), self.precision)
         ev[3].record()
@@ -110,8 +129,8 @@ class FilteredOpw:
         torch.cuda.synchronize()
         if int(self.gram.info.item()):
             raise np.linalg.LinAlgError("cuSOLVER eigendecomposition failed")
-        if self.half and int(self.range_error.item()):
-            raise ValueError("FP16 IQ requires finite components within +/-65504; rescale inputs explicitly")
+        if self.storage != "float32" and int(self.range_error.item()):
+            raise ValueError("packed IQ storage requires finite components (within +/-65504 for FP16)")
         if _lib.device_error():
             raise _lib.RcabeamCudaError("a reconstruction kernel timed out waiting on its staging pipeline")
 
@@ -131,11 +150,12 @@ class FilteredOpw:
         torch.cuda.synchronize()
         return {name: round(self.events[i].elapsed_time(self.events[i + 1]), 3) for i, name in enumerate(_STAGES)}
 
-    @staticmethod
-    def launches_per_step() -> int:
-        # pack x2, voxel order (bbox, morton, 4 radix-sort passes), DAS main + tail,
-        # scale, Gram, finish, projection.
-        return 2 + 6 + 2 + 4
+    def launches_per_step(self) -> int:
+        """Kernels of this library launched per ``run``: pack x2, voxel order (bounding box,
+        Morton codes, 4 radix-sort passes), DAS (one persistent tensor-core launch, or main +
+        tail staged launches), scale, Gram, Gram finish, projection."""
+        das = 1 if self.storage != "float32" and self.channel_shape[3] % 4 == 0 else 2
+        return 2 + 6 + das + 4
 
 
 def synthetic_channels(shape, *, generator: torch.Generator, device, scale: float = 1.0):
