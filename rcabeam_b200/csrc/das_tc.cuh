@@ -1,35 +1,40 @@
 // Tensor-core (tcgen05) RCA delay-and-sum: interpolation as a banded GEMM.
 //
-// For one (aperture, channel, angle) step and a tile of 64 spatially compact
+// For one (aperture, channel, angle) step and a tile of 128 spatially compact
 // voxels, every voxel's two interpolation taps fall in a window of <= 16
-// sample rows.  Writing the taps as a 128 x 16 coefficient matrix A -- row
-// 2v holds Re(phase * (1 - w), phase * w) of voxel v at its window rows,
-// row 2v + 1 the imaginary parts -- the step is
+// sample rows (about 13 on average for the full-size workload).  Writing the
+// taps of a 64-voxel group as a 128 x 16 coefficient matrix A -- row 2v holds
+// Re(phase * (1 - w), phase * w) of voxel v at its window rows, row 2v + 1
+// the imaginary parts -- one step of one group is
 //
 //     D[128, 2F] += A[128, 16] . X[16, 2F]
 //
 // where X is the staged window of packed channel samples with real and
-// imaginary parts interleaved along the frame axis (2F columns).  Lane 2v of
-// the TMEM accumulator then holds P = Re(A) X and lane 2v + 1 holds
-// Q = Im(A) X, and the voxel's IQ is (P_re - Q_im) + j (P_im + Q_re).
-// Accumulating all (aperture, channel, angle) steps in one TMEM accumulator
-// gives the OPW sum; the epilogue adds the power Doppler.
+// imaginary parts interleaved along the frame axis (F frames, 2F <= 256
+// columns).  Lane 2v of the group's TMEM accumulator then holds P = Re(A) X
+// and lane 2v + 1 holds Q = Im(A) X, and the voxel's IQ is
+// (P_re - Q_im) + j (P_im + Q_re).  Both 64-voxel groups of a tile use the
+// same staged window (two MMAs per product), which halves the window bytes
+// per interpolated sample; frames beyond 128 run as further passes.
 //
-// Precision: FP16-packed channels are exact FP16; the coefficients are split
-// into FP16 hi + lo (two MMAs, ~22-bit coefficients).  Float32 channels are
-// pre-split into BF16 hi + lo planes; with BF16 hi/lo coefficients the step
-// uses three MMAs (Ahi Xhi + Alo Xhi + Ahi Xlo).  Accumulation is float32.
+// Precision: FP16-packed channels are exact FP16 and the coefficients are
+// split into FP16 hi + lo (two products, coefficients scaled by 2^10 so the lo
+// halves stay normal).  Float32 channels are pre-split into BF16 hi + lo
+// planes; with BF16 hi/lo coefficients each step runs three products
+// (Ahi Xhi + Alo Xhi + Ahi Xlo).  Accumulation is float32 in TMEM.
 //
-// Roles (224 threads, one CTA per SM, persistent over (tile, frame chunk)):
-//   warps 0-1   builders, one voxel per lane: per tile a table of float64
-//               transmit delays and transmit phases per (aperture, angle), per
-//               channel the float64 receive delay and phase; per step the tap
-//               (sample index, weight, phase by angle addition), the tile's
-//               row window (warp reductions + a named barrier), the A hi/lo
-//               rows (zero fill + two 16-bit stores), and lane 0 of warp 0
-//               issues the window's TMA boxes (64 columns x 16 rows, SWIZZLE_128B);
-//   warp 2      TMEM allocator; lane 0 issues tcgen05.mma and commits;
-//   warps 3-6   epilogue: tcgen05.ld of the accumulator, complex combine,
+// Roles (288 threads, one CTA per SM, persistent over (tile, frame pass)):
+//   warps 0-3   builders.  A warp owns whole steps: channels are dealt round
+//               robin to the warps, so each warp forms the float64 receive
+//               delay and phase of its channel once for the 128 voxels (four
+//               per lane) and then, per angle, the taps (sample index, weight,
+//               phase by angle addition with a per-tile table of transmit
+//               delays and phases), the tile's row window (warp reductions),
+//               the A hi/lo rows of both groups, claims the next ring stage
+//               from a shared counter and stages the window with TMA
+//               (64-column x 16-row SWIZZLE_128B boxes, spread over lanes);
+//   warp 4      TMEM allocator; lane 0 issues tcgen05.mma and commits;
+//   warps 5-8   epilogue: tcgen05.ld of both accumulators, complex combine,
 //               IQ store and power.
 // Shared-memory operands: A is K-major without swizzle (8 x 16-byte core
 // matrices; LBO = 128 B between the two K cores, SBO = 256 B between 8-row
@@ -45,15 +50,17 @@
 namespace rcb {
 namespace tc {
 
-constexpr int kVox = 64;
+constexpr int kVox = 128;          // voxels per tile
+constexpr int kGroupVox = 64;      // voxels per M=128 MMA block
 constexpr int kRows = 16;
 constexpr int kStages = 4;
 constexpr int kBoxCols = 64;       // 16-bit columns per TMA box (one 128-byte swizzle atom)
 constexpr int kBoxBytes = kBoxCols * 2 * kRows;  // 2048
-constexpr int kMaxFrames = 256;    // frames per pass: 2 x frames float32 TMEM columns <= 512
-constexpr int kThreads = 224;
-constexpr int kBuilders = 2;  // builder warps (64 lanes = 64 voxels)
-constexpr int kTmemCols = 512;
+constexpr int kMaxFrames = 128;    // frames per pass: 2 x frames columns <= 256 per group
+constexpr int kBuilders = 4;       // builder warps
+constexpr int kMmaWarp = kBuilders;
+constexpr int kThreads = (kBuilders + 1 + 4) * 32;
+constexpr int kTmemCols = 512;     // group g accumulates in columns [256 g, 256 g + 2F)
 constexpr int kAMatBytes = 128 * kRows * 2;  // 4096: one 128 x 16 16-bit matrix
 // FP16 coefficients (|c| <= 1) are scaled by 2^10 before the hi/lo split so that
 // the lo halves of small coefficients stay out of the FP16 subnormal range; the
@@ -75,7 +82,7 @@ struct Args {
   float2* signal;
   int ns, nc, na, nt, nv;
   double c, fs, fd, fn;
-  int frames;      // frames per pass (multiple of 8, <= 256)
+  int frames;      // frames per pass (multiple of 8, <= 128)
   int chunks;      // passes per tile
   int ncols;       // 2 * frames
   int nbox;        // TMA boxes per plane
@@ -86,11 +93,15 @@ struct Args {
 template <bool BF16X3>
 struct Layout {
   static constexpr int kPlanes = BF16X3 ? 2 : 1;
-  __host__ __device__ static size_t stage_bytes(int nbox) { return 2 * kAMatBytes + size_t(kPlanes) * nbox * kBoxBytes; }
-  // stages | control (barriers, meta, TMEM slot, window exchange) | angle table |
-  // per-tile transmit delays [2][na][64] double | transmit phases [2][na][64] float2
+  // A: [group][hi, lo] matrices; then the planes' boxes.
+  __host__ __device__ static size_t stage_bytes(int nbox) {
+    return 4 * kAMatBytes + size_t(kPlanes) * nbox * kBoxBytes;
+  }
+  // stages | control (barriers, meta, counter, TMEM slot) | angle table |
+  // per-tile transmit delays [2][na][128] double | transmit phases [2][na][128] float2
   static size_t bytes(int nbox, int na) {
-    return kStages * stage_bytes(nbox) + 1024 + size_t(na) * 3 * sizeof(double) + size_t(na) * 2 * 64 * 16 + 1024;
+    return kStages * stage_bytes(nbox) + 1024 + size_t(na) * 3 * sizeof(double) + size_t(na) * 2 * kVox * 16 +
+           1024;
   }
 };
 
@@ -188,8 +199,6 @@ __device__ __forceinline__ void put_row(unsigned char* a_hi, unsigned char* a_lo
   }
 }
 
-__device__ __forceinline__ void builders_sync() { asm volatile("bar.sync 1, %0;" ::"r"(kBuilders * 32) : "memory"); }
-
 // exp(+j 2 pi fd tau) with the cycle count reduced in float64.
 __device__ __forceinline__ float2 demod_phase(double fd, double tau) {
   double cyc = fd * tau;
@@ -205,6 +214,7 @@ __global__ void __launch_bounds__(kThreads, 1)
            const __grid_constant__ CUtensorMap map_rc_lo, const __grid_constant__ CUtensorMap map_cr_lo, Args p) {
   using L = Layout<BF16X3>;
   constexpr int kPlanes = L::kPlanes;
+  constexpr int kProducts = BF16X3 ? 3 : 2;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // Align the working area to 1024 bytes (SWIZZLE_128B atoms).
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -218,20 +228,22 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* drain = acc_empty + 1;
   int* meta = reinterpret_cast<int*>(drain + 1);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(meta + kStages);
-  int* xch = reinterpret_cast<int*>(ctrl + 512);  // [parity][builder warp][lo, hi]
+  int* counter = reinterpret_cast<int*>(tmem_slot + 1);  // next ring stage to claim
+  int* item_steps = counter + 1;                         // steps staged for the current item
   double* angle_tab = reinterpret_cast<double*>(ctrl + 1024);
-  double* tx_delay = angle_tab + 3 * p.na;                                   // [2][na][64]
-  float2* tx_phase = reinterpret_cast<float2*>(tx_delay + 2 * p.na * kVox);  // [2][na][64]
+  double* tx_delay = angle_tab + 3 * p.na;                                   // [2][na][128]
+  float2* tx_phase = reinterpret_cast<float2*>(tx_delay + 2 * p.na * kVox);  // [2][na][128]
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full[s], kBuilders * 32);
-      mbar_init(&empty[s], 1);
+      mbar_init(&full[s], 32);  // the writing builder warp
+      mbar_init(&empty[s], 1);  // tcgen05.commit (or a plain arrive for markers)
     }
     mbar_init(acc_full, 1);
     mbar_init(acc_empty, 4);
     mbar_init(drain, 1);
+    *counter = 0;
     fence_mbar_init();
   }
   for (int a = threadIdx.x; a < p.na; a += blockDim.x) {
@@ -240,7 +252,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     angle_tab[3 * a + 1] = sin(th);
     angle_tab[3 * a + 2] = double(p.starts[a]);
   }
-  if (warp == kBuilders) {
+  if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(kTmemCols)
                  : "memory");
@@ -254,9 +266,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (warp < kBuilders) {
     // ----------------------------------------------------------- builders --
-    const int v = 32 * warp + lane;  // voxel slot owned by this lane
-    const bool leader = warp == 0 && lane == 0;
-    if (leader) {
+    if (warp == 0 && lane == 0) {
       prefetch_tensormap(&map_rc_hi);
       prefetch_tensormap(&map_cr_hi);
       if constexpr (BF16X3) {
@@ -264,176 +274,202 @@ __global__ void __launch_bounds__(kThreads, 1)
         prefetch_tensormap(&map_cr_lo);
       }
     }
-    uint32_t k = 0, parity = 0;
     bool ok = true;
     const uint32_t tx_bytes = uint32_t(kPlanes * p.nbox * kBoxBytes);
     const float sc = kCoefScale<BF16X3>;
-    // Waits for stage k to be free (uniform within a warp).  After a failed wait a
-    // builder stops waiting and writing but keeps executing the loops, so both
-    // builder warps always meet the same named barriers.
-    auto acquire = [&](int s) -> bool {
-      return __all_sync(0xffffffffu, mbar_wait(&empty[s], ((k / kStages) & 1) ^ 1, p.err, kErrWaitEmpty));
+    auto builders_sync = [] { asm volatile("bar.sync 1, %0;" ::"n"(kBuilders * 32) : "memory"); };
+    // Claims the next ring stage (uniform in the warp) and waits until it is free.
+    auto claim = [&](uint32_t& k) -> bool {
+      uint32_t mine = 0;
+      if (lane == 0) mine = uint32_t(atomicAdd(counter, 1));
+      k = __shfl_sync(0xffffffffu, mine, 0);
+      return __all_sync(0xffffffffu,
+                        mbar_wait(&empty[k % kStages], ((k / kStages) & 1) ^ 1, p.err, kErrWaitEmpty));
     };
-    auto issue_tma = [&](unsigned char* stage, const CUtensorMap* mh, const CUtensorMap* ml, int col0, int row,
-                         int slab, int s) {
-      mbar_arrive_expect_tx(&full[s], tx_bytes);
-      unsigned char* b0 = stage + 2 * kAMatBytes;
-      for (int bx = 0; bx < p.nbox; ++bx) tma_load_3d(b0 + bx * kBoxBytes, mh, &full[s], col0 + bx * kBoxCols, row, slab);
-      if constexpr (BF16X3) {
-        unsigned char* b1 = b0 + p.nbox * kBoxBytes;
-        for (int bx = 0; bx < p.nbox; ++bx)
-          tma_load_3d(b1 + bx * kBoxBytes, ml, &full[s], col0 + bx * kBoxCols, row, slab);
+    // Stages the window [row, row + 16) x [col0, col0 + ncols) of every plane.
+    auto stage_window = [&](uint32_t s, unsigned char* stage, int config, int col0, int row, int slab) {
+      const CUtensorMap* mh = config ? &map_cr_hi : &map_rc_hi;
+      const CUtensorMap* ml = config ? &map_cr_lo : &map_rc_lo;
+      if (lane == 0) mbar_arrive_expect_tx(&full[s], tx_bytes);
+      __syncwarp();
+      unsigned char* b0 = stage + 4 * kAMatBytes;
+      if (lane < kPlanes * p.nbox) {
+        const bool second = lane >= p.nbox;
+        const int j = second ? lane - p.nbox : lane;
+        tma_load_3d(b0 + (second ? p.nbox : 0) * kBoxBytes + j * kBoxBytes, second ? ml : mh, &full[s],
+                    col0 + j * kBoxCols, row, slab);
       }
+      if (lane != 0) mbar_arrive(&full[s]);
     };
     for (int item = blockIdx.x; item < work_items; item += gridDim.x) {
       const int tile = item / p.chunks, chunk = item % p.chunks;
       const int col0 = 2 * chunk * p.frames;
-      int steps = 0;
-      const size_t qv = size_t(tile) * kVox + v;
-      const unsigned vid = qv < size_t(p.nv) ? (p.order ? p.order[qv] : unsigned(qv)) : UINT_MAX;
-      const bool valid = vid != UINT_MAX;
-      const size_t b3 = valid ? 3 * size_t(vid) : 0;
-      const double px = valid ? double(p.scan[b3]) : 0.0;
-      const double pz = valid ? double(p.scan[b3 + 1]) : 0.0;
-      const double py = valid ? double(p.scan[b3 + 2]) : 0.0;
-      // Per-tile transmit table (each lane reads back only its own entries).
-      for (int config = 0; config < 2; ++config) {
-        for (int a = 0; a < p.na; ++a) {
-          double ttx = transmit_delay(config ? px : py, pz, angle_tab[3 * a], angle_tab[3 * a + 1], p.c);
-          tx_delay[(config * p.na + a) * kVox + v] = ttx;
-          tx_phase[(config * p.na + a) * kVox + v] = demod_phase(p.fd, ttx);
-        }
+      // Voxels of this lane: slots lane + 32 j (group = slot / 64).
+      double px[4], pz[4], py[4];
+      bool pv[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const size_t q = size_t(tile) * kVox + lane + 32 * j;
+        const unsigned v = q < size_t(p.nv) ? (p.order ? p.order[q] : unsigned(q)) : UINT_MAX;
+        pv[j] = v != UINT_MAX;
+        const size_t b3 = pv[j] ? 3 * size_t(v) : 0;
+        px[j] = pv[j] ? double(p.scan[b3]) : 0.0;
+        pz[j] = pv[j] ? double(p.scan[b3 + 1]) : 0.0;
+        py[j] = pv[j] ? double(p.scan[b3 + 2]) : 0.0;
       }
+      // Per-tile transmit table, filled cooperatively by the builder warps.
+      builders_sync();  // previous item's table reads are complete
+      for (int e = warp * 32 + lane; e < 2 * p.na * kVox; e += kBuilders * 32) {
+        const int v = e % kVox, ca = e / kVox, config = ca / p.na, a = ca % p.na;
+        const size_t q = size_t(tile) * kVox + v;
+        const unsigned vid = q < size_t(p.nv) ? (p.order ? p.order[q] : unsigned(q)) : UINT_MAX;
+        const size_t b3 = vid != UINT_MAX ? 3 * size_t(vid) : 0;
+        const double x = vid != UINT_MAX ? double(p.scan[b3]) : 0.0;
+        const double z = vid != UINT_MAX ? double(p.scan[b3 + 1]) : 0.0;
+        const double y = vid != UINT_MAX ? double(p.scan[b3 + 2]) : 0.0;
+        const double ttx = transmit_delay(config ? x : y, z, angle_tab[3 * a], angle_tab[3 * a + 1], p.c);
+        tx_delay[e] = ttx;
+        tx_phase[e] = demod_phase(p.fd, ttx);
+      }
+      builders_sync();
+      int steps = 0;
       for (int config = 0; config < 2; ++config) {
         const float* el = config ? p.ye : p.xe;
-        const CUtensorMap* mh = config ? &map_cr_hi : &map_rc_hi;
-        const CUtensorMap* ml = config ? &map_cr_lo : &map_rc_lo;
-        for (int ch = 0; ch < p.nc; ++ch) {
-          bool act;
-          const double trx = receive_delay(config ? py : px, pz, double(el[ch]), p.c, p.fn, &act);
-          act = act && valid;
-          const float2 ph_rx = demod_phase(p.fd, trx);
+        for (int ch = warp; ch < p.nc; ch += kBuilders) {
+          double trx[4];
+          float2 ph_rx[4];
+          bool act[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            trx[j] = receive_delay(config ? py[j] : px[j], pz[j], double(el[ch]), p.c, p.fn, &act[j]);
+            act[j] = act[j] && pv[j];
+            ph_rx[j] = demod_phase(p.fd, trx[j]);
+          }
           for (int a = 0; a < p.na; ++a) {
-            const int ti = (config * p.na + a) * kVox + v;
-            const double tau = __dadd_rn(tx_delay[ti], trx);
-            const double sample = __dmul_rn(__dadd_rn(tau, -angle_tab[3 * a + 2]), p.fs);
-            const bool in_window = act && sample >= 0.0 && sample <= double(p.ns - 1);
-            const double fl = floor(sample);
-            const int i0 = in_window ? int(fl) : -1;
-            const float w = float(sample - fl);
-            // Window of the 64 voxels: warp reductions, exchanged between the two warps.
-            int lo = __reduce_min_sync(0xffffffffu, i0 >= 0 ? i0 : INT_MAX);
-            int hi = __reduce_max_sync(0xffffffffu, i0);
-            if (lane == 0) {
-              xch[(parity * kBuilders + warp) * 2] = lo;
-              xch[(parity * kBuilders + warp) * 2 + 1] = hi;
+            const double start = angle_tab[3 * a + 2];
+            int i0[4];
+            float w[4];
+            int lo = INT_MAX, hi = -1;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const int ti = (config * p.na + a) * kVox + lane + 32 * j;
+              const double sample = __dmul_rn(__dadd_rn(__dadd_rn(tx_delay[ti], trx[j]), -start), p.fs);
+              const bool in_window = act[j] && sample >= 0.0 && sample <= double(p.ns - 1);
+              const double fl = floor(sample);
+              i0[j] = in_window ? int(fl) : -1;
+              w[j] = float(sample - fl);
+              if (i0[j] >= 0) {
+                lo = min(lo, i0[j]);
+                hi = max(hi, i0[j]);
+              }
             }
-            builders_sync();
-            lo = min(xch[parity * kBuilders * 2], xch[parity * kBuilders * 2 + 2]);
-            hi = max(xch[parity * kBuilders * 2 + 1], xch[parity * kBuilders * 2 + 3]);
-            parity ^= 1;
+            lo = __reduce_min_sync(0xffffffffu, lo);
+            hi = __reduce_max_sync(0xffffffffu, hi);
             if (lo == INT_MAX) continue;  // no voxel of the tile sees this slab
-            const float2 pt = tx_phase[ti];
-            const float2 ph = make_float2(pt.x * ph_rx.x - pt.y * ph_rx.y, pt.x * ph_rx.y + pt.y * ph_rx.x);
-            // Coefficients of x[i0] and x[i0 + 1]: phase * (1 - w) and phase * w (scaled).
-            const float2 c0 = make_float2(sc * ph.x * (1.f - w), sc * ph.y * (1.f - w));
-            const float2 c1 = make_float2(sc * ph.x * w, sc * ph.y * w);
+            float2 c0[4], c1[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const float2 pt = tx_phase[(config * p.na + a) * kVox + lane + 32 * j];
+              const float2 ph = make_float2(pt.x * ph_rx[j].x - pt.y * ph_rx[j].y, pt.x * ph_rx[j].y + pt.y * ph_rx[j].x);
+              // Coefficients of x[i0] and x[i0 + 1]: phase * (1 - w) and phase * w (scaled).
+              c0[j] = make_float2(sc * ph.x * (1.f - w[j]), sc * ph.y * (1.f - w[j]));
+              c1[j] = make_float2(sc * ph.x * w[j], sc * ph.y * w[j]);
+            }
             const int slab = ch * p.na + a;
             for (int base = lo; base <= hi; base += kRows - 1) {
-              const int s = k % kStages;
-              if (ok) ok = acquire(s);
-              if (!ok) continue;  // failed: keep the barrier sequence, skip the work
+              uint32_t k = 0;
+              if (ok) ok = claim(k);
+              if (!ok) continue;  // failed: keep the control flow, skip the work
+              const uint32_t s = k % kStages;
               unsigned char* stage = stages + size_t(s) * stage_bytes;
-              const int r = i0 - base;
-              const int rr = (i0 >= 0 && r >= 0 && r < kRows - 1) ? r : -1;
-              put_row<BF16X3>(stage, stage + kAMatBytes, 2 * v, rr, c0.x, c1.x);
-              put_row<BF16X3>(stage, stage + kAMatBytes, 2 * v + 1, rr, c0.y, c1.y);
-              if (leader) meta[s] = kStep;
+#pragma unroll
+              for (int j = 0; j < 4; ++j) {
+                const int r = i0[j] - base;
+                const int rr = (i0[j] >= 0 && r >= 0 && r < kRows - 1) ? r : -1;
+                const int g = j >> 1;                          // slots 0-63 -> group 0, 64-127 -> group 1
+                const int m = 2 * (lane + 32 * (j & 1));       // A row of the voxel within its group
+                unsigned char* a_hi = stage + (2 * g) * kAMatBytes;
+                unsigned char* a_lo = a_hi + kAMatBytes;
+                put_row<BF16X3>(a_hi, a_lo, m, rr, c0[j].x, c1[j].x);
+                put_row<BF16X3>(a_hi, a_lo, m + 1, rr, c0[j].y, c1[j].y);
+              }
+              if (lane == 0) meta[s] = kStep;
               fence_async_smem();
-              if (leader)
-                issue_tma(stage, mh, ml, col0, base, slab, s);
-              else
-                mbar_arrive(&full[s]);
-              ++k;
+              stage_window(s, stage, config, col0, base, slab);
               ++steps;
             }
           }
         }
       }
-      if (ok && steps == 0) {
-        // No voxel of the tile sees any sample: one all-zero step (zero
-        // coefficients; window beyond the last sample, which TMA fills with
-        // zeros) so that the accumulator is still initialized.
-        const int s = k % kStages;
-        if (ok) ok = acquire(s);
-        if (ok) {
-          unsigned char* stage = stages + size_t(s) * stage_bytes;
-          put_row<BF16X3>(stage, stage + kAMatBytes, 2 * v, -1, 0.f, 0.f);
-          put_row<BF16X3>(stage, stage + kAMatBytes, 2 * v + 1, -1, 0.f, 0.f);
-          if (leader) meta[s] = kStep;
-          fence_async_smem();
-          if (leader)
-            issue_tma(stage, &map_rc_hi, &map_rc_lo, col0, p.ns, 0, s);
-          else
-            mbar_arrive(&full[s]);
-          ++k;
-        }
-      }
-      // End of this work item.
-      if (ok) {
-        const int s = k % kStages;
-        if (ok) ok = acquire(s);
-        if (ok) {
-          if (leader) meta[s] = kTileEnd;
-          mbar_arrive(&full[s]);
-          ++k;
-        }
-      }
-      // The transmit table is rewritten for the next item only after both warps are done with it.
+      // Every builder's steps of this item are staged before its markers.
       builders_sync();
-    }
-    if (ok) {
-      const int s = k % kStages;
-      if (ok) ok = acquire(s);
-      if (ok) {
-        if (leader) meta[s] = kFinish;
-        mbar_arrive(&full[s]);
-        ++k;
+      if (warp == 0 && lane == 0) *item_steps = 0;
+      builders_sync();
+      if (lane == 0) atomicAdd(item_steps, steps);
+      builders_sync();
+      if (warp == 0) {
+        if (*item_steps == 0) {
+          // No voxel of the tile sees any sample: one all-zero step (zero
+          // coefficients; window beyond the last sample, which TMA fills with
+          // zeros) so that the accumulators are still initialized.
+          uint32_t k = 0;
+          if (ok) ok = claim(k);
+          if (ok) {
+            const uint32_t s = k % kStages;
+            unsigned char* stage = stages + size_t(s) * stage_bytes;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const int g = j >> 1, m = 2 * (lane + 32 * (j & 1));
+              put_row<BF16X3>(stage + 2 * g * kAMatBytes, stage + (2 * g + 1) * kAMatBytes, m, -1, 0.f, 0.f);
+              put_row<BF16X3>(stage + 2 * g * kAMatBytes, stage + (2 * g + 1) * kAMatBytes, m + 1, -1, 0.f, 0.f);
+            }
+            if (lane == 0) meta[s] = kStep;
+            fence_async_smem();
+            stage_window(s, stage, 0, col0, p.ns, 0);
+          }
+        }
+        uint32_t k = 0;
+        if (ok) ok = claim(k);
+        if (ok) {
+          if (lane == 0) meta[k % kStages] = kTileEnd;
+          mbar_arrive(&full[k % kStages]);
+        }
       }
     }
-    // Drain: every issued copy has landed before the builders leave.
-    for (uint32_t u = k > kStages ? k - kStages : 0; u < k; ++u)
-      mbar_wait(&full[u % kStages], (u / kStages) & 1, p.err, kErrWaitDrain);
-  } else if (warp == kBuilders) {
+    builders_sync();  // every builder's claims are done
+    if (warp == 0) {
+      uint32_t k = 0;
+      if (ok) ok = claim(k);
+      if (ok) {
+        if (lane == 0) meta[k % kStages] = kFinish;
+        mbar_arrive(&full[k % kStages]);
+      }
+      // Drain: the copies of the last stages (globally last, so no later phase
+      // exists on their barriers) have landed before the builders leave.
+      const uint32_t total = uint32_t(*counter);
+      for (uint32_t u = total > kStages ? total - kStages : 0; u < total; ++u)
+        mbar_wait(&full[u % kStages], (u / kStages) & 1, p.err, kErrWaitDrain);
+    }
+  } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------------- MMA --
     if (lane == 0) {
-      const uint32_t n0 = p.ncols < 256 ? uint32_t(p.ncols) : 256u;
-      const uint32_t n1 = uint32_t(p.ncols) - n0;  // second part (0 if ncols <= 256)
-      const uint32_t id0 = instr_desc(BF16X3, 128, int(n0));
-      const uint32_t id1 = n1 ? instr_desc(BF16X3, 128, int(n1)) : 0u;
+      const uint32_t idesc = instr_desc(BF16X3, 128, p.ncols);
       uint32_t k = 0, tiles_done = 0;
-      bool started = false;  // the current tile owns the accumulator
-      bool issued = false;   // the current tile has issued an MMA
-      bool ok = true;
+      bool started = false;  // the current item owns the accumulators
+      bool issued = false;   // the current item has issued an MMA
       for (;;) {
         const int s = k % kStages;
-        if (!mbar_wait(&full[s], (k / kStages) & 1, p.err, kErrWaitFull)) {
-          ok = false;
-          break;
-        }
+        if (!mbar_wait(&full[s], (k / kStages) & 1, p.err, kErrWaitFull)) break;
         const int m = meta[s];
         if (m == kFinish) break;
         if (!started) {
-          // The previous tile's epilogue must have drained the accumulator.
-          if (tiles_done > 0 && !mbar_wait(acc_empty, (tiles_done - 1) & 1, p.err, kErrWaitEmpty)) {
-            ok = false;
-            break;
-          }
+          // The previous item's epilogue must have drained the accumulators.
+          if (tiles_done > 0 && !mbar_wait(acc_empty, (tiles_done - 1) & 1, p.err, kErrWaitEmpty)) break;
           started = true;
         }
         tc_fence_after();
         if (m == kTileEnd) {
-          mma_commit(acc_full);  // arrives once this tile's MMAs have completed
+          mma_commit(acc_full);  // arrives once this item's MMAs have completed
           mbar_arrive(&empty[s]);
           ++k;
           ++tiles_done;
@@ -442,18 +478,18 @@ __global__ void __launch_bounds__(kThreads, 1)
           continue;
         }
         const uint32_t st = smem_u32(stages + size_t(s) * stage_bytes);
-        const uint32_t a_hi = st, a_lo = st + kAMatBytes, b_hi = st + 2 * kAMatBytes;
+        const uint32_t b_hi = st + 4 * kAMatBytes;
         const uint32_t b_lo = b_hi + uint32_t(p.nbox * kBoxBytes);
-        // Products: Ahi Xhi, Alo Xhi (+ Ahi Xlo for BF16 x3).
-        constexpr int kProducts = BF16X3 ? 3 : 2;
 #pragma unroll
-        for (int q = 0; q < kProducts; ++q) {
-          const uint32_t a = q == 1 ? a_lo : a_hi;
-          const uint32_t b = q == 2 ? b_lo : b_hi;
-          const uint64_t ad = smem_desc(a, 128, 256, kLayoutNone);
-          const uint32_t acc = (issued || q > 0) ? 1u : 0u;
-          mma_f16(tmem, ad, smem_desc(b, kBoxBytes, 1024, kLayoutSw128), id0, acc);
-          if (n1) mma_f16(tmem + 256, ad, smem_desc(b + 4 * kBoxBytes, kBoxBytes, 1024, kLayoutSw128), id1, acc);
+        for (int g = 0; g < 2; ++g) {
+          const uint32_t a_hi = st + 2 * g * kAMatBytes, a_lo = a_hi + kAMatBytes;
+#pragma unroll
+          for (int q = 0; q < kProducts; ++q) {
+            const uint32_t a = q == 1 ? a_lo : a_hi;
+            const uint32_t b = q == 2 ? b_lo : b_hi;
+            mma_f16(tmem + 256u * g, smem_desc(a, 128, 256, kLayoutNone), smem_desc(b, kBoxBytes, 1024, kLayoutSw128),
+                    idesc, (issued || q > 0) ? 1u : 0u);
+          }
         }
         issued = true;
         mma_commit(&empty[s]);  // frees the stage once these MMAs have read it
@@ -462,43 +498,43 @@ __global__ void __launch_bounds__(kThreads, 1)
       // Every issued MMA has completed before the warp leaves (TMEM is freed after).
       mma_commit(drain);
       mbar_wait(drain, 0, p.err, kErrWaitDrain);
-      (void)ok;
     }
     __syncwarp();
   } else {
     // ----------------------------------------------------------- epilogue --
     const int q = warp & 3;  // TMEM lane quarter this warp may access
     const int m = 32 * q + lane;
-    const int v_slot = m >> 1;
     const bool is_p = (m & 1) == 0;
     uint32_t tiles_done = 0;
     for (int item = blockIdx.x; item < work_items; item += gridDim.x) {
       const int tile = item / p.chunks, chunk = item % p.chunks;
       if (!__all_sync(0xffffffffu, mbar_wait(acc_full, tiles_done & 1, p.err, kErrWaitFull))) break;
       tc_fence_after();
-      size_t qv = size_t(tile) * kVox + v_slot;
-      const unsigned v = qv < size_t(p.nv) ? (p.order ? p.order[qv] : unsigned(qv)) : UINT_MAX;
       const int f0 = chunk * p.frames;
-      float power = 0.f;
-      for (int c0 = 0; c0 < p.ncols; c0 += 32) {
-        float val[32];
-        tmem_ld32(tmem + (uint32_t(32 * q) << 16) + uint32_t(c0), val);
-        // Partner lane holds the other half (P <-> Q) of the same voxel.
+      for (int g = 0; g < 2; ++g) {
+        const size_t qv = size_t(tile) * kVox + kGroupVox * g + (m >> 1);
+        const unsigned v = qv < size_t(p.nv) ? (p.order ? p.order[qv] : unsigned(qv)) : UINT_MAX;
+        float power = 0.f;
+        for (int c0 = 0; c0 < p.ncols; c0 += 32) {
+          float val[32];
+          tmem_ld32(tmem + (uint32_t(32 * q) << 16) + 256u * g + uint32_t(c0), val);
+          // The partner lane holds the other half (P <-> Q) of the same voxel.
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          float other_re = __shfl_xor_sync(0xffffffffu, val[2 * i], 1);
-          float other_im = __shfl_xor_sync(0xffffffffu, val[2 * i + 1], 1);
-          // P lane: D = (P_re - Q_im, P_im + Q_re).
-          float dre = (val[2 * i] - other_im) * (1.0f / kCoefScale<BF16X3>);
-          float dim = (val[2 * i + 1] + other_re) * (1.0f / kCoefScale<BF16X3>);
-          int frame = f0 + (c0 >> 1) + i;
-          if (is_p && v != UINT_MAX && frame < p.nt && frame < f0 + p.frames) {
-            if (p.signal) p.signal[size_t(v) * p.nt + frame] = make_float2(dre, dim);
-            power += dre * dre + dim * dim;
+          for (int i = 0; i < 16; ++i) {
+            const float other_re = __shfl_xor_sync(0xffffffffu, val[2 * i], 1);
+            const float other_im = __shfl_xor_sync(0xffffffffu, val[2 * i + 1], 1);
+            // P lane: D = (P_re - Q_im, P_im + Q_re).
+            const float dre = (val[2 * i] - other_im) * (1.0f / kCoefScale<BF16X3>);
+            const float dim = (val[2 * i + 1] + other_re) * (1.0f / kCoefScale<BF16X3>);
+            const int frame = f0 + (c0 >> 1) + i;
+            if (is_p && v != UINT_MAX && frame < p.nt && frame < f0 + p.frames) {
+              if (p.signal) p.signal[size_t(v) * p.nt + frame] = make_float2(dre, dim);
+              power += dre * dre + dim * dim;
+            }
           }
         }
+        if (is_p && v != UINT_MAX) atomicAdd(p.pd + 2 * size_t(v), power / float(p.nt));
       }
-      if (is_p && v != UINT_MAX) atomicAdd(p.pd + 2 * size_t(v), power / float(p.nt));
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(acc_empty);
@@ -506,7 +542,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   }
   __syncthreads();
-  if (warp == kBuilders) {
+  if (warp == kMmaWarp) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
   }

@@ -245,10 +245,22 @@ static bool tc_eligible(const void* const* planes, int count, size_t nt) {
   return true;
 }
 
-// Tensor-core OPW over all (tile, frame chunk) work items with one persistent CTA per SM.
+// Shared memory of the tensor-core OPW for nt frames and na angles (0 if it cannot run).
+static size_t tc_smem_bytes(bool bf16x3, size_t nt, size_t na) {
+  const size_t chunks = (nt + tc::kMaxFrames - 1) / tc::kMaxFrames;
+  const size_t frames = ((nt + chunks - 1) / chunks + 7) / 8 * 8;
+  const int nbox = int((2 * frames + tc::kBoxCols - 1) / tc::kBoxCols);
+  size_t smem = (bf16x3 ? tc::Layout<true>::bytes(nbox, int(na)) : tc::Layout<false>::bytes(nbox, int(na))) + 1024;
+  if (smem < 120 * 1024) smem = 120 * 1024;  // one CTA per SM: each owns all 512 TMEM columns
+  return smem <= 227 * 1024 ? smem : 0;
+}
+
+// Tensor-core OPW over all (tile, frame pass) work items with one persistent CTA per SM.
 template <bool BF16X3>
 static rcabeam_status run_tc(tc::Args a) {
   const size_t nt = size_t(a.nt);
+  const size_t smem = tc_smem_bytes(BF16X3, nt, size_t(a.na));
+  if (!smem) return RCABEAM_ERROR_ARGUMENT;
   a.chunks = int((nt + tc::kMaxFrames - 1) / tc::kMaxFrames);
   int frames = int((nt + a.chunks - 1) / a.chunks);
   frames = (frames + 7) / 8 * 8;
@@ -269,9 +281,6 @@ static rcabeam_status run_tc(tc::Args a) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  size_t smem = tc::Layout<BF16X3>::bytes(a.nbox, a.na) + 1024;
-  // Keep one CTA per SM: each CTA owns all 512 TMEM columns.
-  if (smem < 120 * 1024) smem = 120 * 1024;
   auto kern = tc::opw_tc<BF16X3>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
     return RCABEAM_ERROR_CUDA;
@@ -336,7 +345,7 @@ static rcabeam_status ensemble_impl(const void* rc, const void* cr, const float*
   a.order = voxel_order(scan, nv, geometry_workspace, 2 * nv * (nc + na) * 16);
   const size_t ntiles = (nv + das::kTileVoxels - 1) / das::kTileVoxels;
   const void* planes[2] = {rc, cr};
-  if (HALF && tc_eligible(planes, 2, nt) && nv <= size_t(INT32_MAX) - tc::kVox) {
+  if (HALF && tc_eligible(planes, 2, nt) && nv <= size_t(INT32_MAX) - tc::kVox && tc_smem_bytes(false, nt, na)) {
     tc::Args t{};
     t.x_hi[0] = rc;
     t.x_hi[1] = cr;
