@@ -207,6 +207,20 @@ rcabeam_status rcabeam_project_device(const void* iq, void* out, double* power, 
  * buffer of this size may be passed instead of the documented one. */
 rcabeam_status rcabeam_ensemble_workspace_bytes(size_t nv, size_t nc, size_t na, size_t* bytes);
 
+/* Same computation as rcabeam_ensemble_device (methods 0, 1, 2, 3 and 5), for
+ * callers that cannot allocate device memory: it takes no geometry workspace
+ * and keeps its scratch in a fixed 8 MiB array inside the library, so the call
+ * itself never allocates.  No counterpart in the reference interface.
+ * Limits: nv <= 262144 voxels per call (RCABEAM_ERROR_ARGUMENT beyond, and for
+ * method 4).  All calls on a device share the scratch: calls that overlap on
+ * the GPU (other streams or threads) race.  The first call on each device
+ * looks up the scratch address; make that first call before any stream
+ * capture.  Launches use the legacy default stream. */
+rcabeam_status rcabeam_ensemble_static_device(const void* rc, const void* cr, const float* scan, const float* xe,
+                                              const float* ye, const float* angles, const float* starts, float* pd,
+                                              void* signal, size_t ns, size_t nc, size_t na, size_t nt, size_t nv,
+                                              float c, float fs, float fd, float fn, int method);
+
 /* Reads and clears the device error word set by a kernel whose bounded wait
  * gave up (0 = no error).  Synchronizes the device. */
 rcabeam_status rcabeam_device_error(int* code);

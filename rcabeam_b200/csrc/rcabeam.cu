@@ -448,6 +448,94 @@ static void project_dispatch(const void* iq, void* out, double* power, size_t ro
   else launch_project<IN, 16>(iq, out, power, rows, nt, vec, k, mode);
 }
 
+// ---------------------------------------------- no-allocation entry point --
+// Some callers cannot call cudaMalloc at all: code running inside a CUDA graph
+// they are recording, real-time acquisition loops whose memory budget is fixed
+// up front, or hosts whose allocator is owned by another runtime.  For them
+// rcabeam_ensemble_static_device keeps its scratch (the voxel traversal-order
+// sort: keys, values, bounding box and radix-sort temporaries) in this
+// file-scope device array instead of a caller-provided workspace.  Every GPU
+// that loads the library holds the array until the process exits, and every
+// call on a device shares it.
+constexpr size_t kStaticMaxVoxels = size_t(1) << 18;       // 262144 voxels per call
+constexpr size_t kStaticScratchBytes = size_t(8) << 20;    // 8 MiB per device
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+// Device address of g_static_scratch for the current device.  The host-side
+// symbol is only a stand-in, so the address is looked up once per device with
+// that device current (the first call on each device does this; make that
+// first call before any stream capture).
+static void* static_scratch_address() {
+  static std::mutex lock;
+  static void* addresses[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> guard(lock);
+  if (!addresses[dev]) {
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_static_scratch) != cudaSuccess) return nullptr;
+    addresses[dev] = ptr;
+  }
+  return addresses[dev];
+}
+
+static rcabeam_status ensemble_static(const void* rc, const void* cr, const float* scan, const float* xe,
+                                      const float* ye, const float* angles, const float* starts, float* pd,
+                                      void* signal, size_t ns, size_t nc, size_t na, size_t nt, size_t nv, float c,
+                                      float fs, float fd, float fn, int method) {
+  if (!rc || !cr || !scan || !xe || !ye || !angles || !starts || !pd || ns < 2 || !nc || !na || !nt || !nv ||
+      c <= 0 || fs <= 0 || !std::isfinite(c) || !std::isfinite(fs) || !std::isfinite(fd) || !std::isfinite(fn))
+    return RCABEAM_ERROR_ARGUMENT;
+  if (method < 0 || method > 5 || method == 4 || (method == 5 && !signal)) return RCABEAM_ERROR_ARGUMENT;
+  if (nv > kStaticMaxVoxels || ns > INT32_MAX || nc > INT32_MAX || na > INT32_MAX || nt > INT32_MAX ||
+      nc * na > INT32_MAX || na > 4096)
+    return RCABEAM_ERROR_ARGUMENT;
+  void* scratch = static_scratch_address();
+  if (!scratch) return RCABEAM_ERROR_CUDA;
+  if (cudaMemsetAsync(pd, 0, 2 * nv * sizeof(float), 0) != cudaSuccess) return RCABEAM_ERROR_CUDA;
+  das::Args a{};
+  a.rc = rc;
+  a.cr = cr;
+  a.scan = scan;
+  a.xe = xe;
+  a.ye = ye;
+  a.angles = angles;
+  a.starts = starts;
+  a.pd = pd;
+  a.signal = static_cast<float2*>(signal);
+  a.ns = int(ns);
+  a.nc = int(nc);
+  a.na = int(na);
+  a.nt = int(nt);
+  a.nv = int(nv);
+  a.c = double(c);
+  a.fs = double(fs);
+  a.fd = double(fd);
+  a.fn = double(fn);
+  a.err = device_error_ptr();
+  if (method == 2 || method == 3) {
+    dim3 grid(unsigned((nv + generic::kWarps - 1) / generic::kWarps),
+              unsigned((nt + 32 * generic::kRegFrames - 1) / (32 * generic::kRegFrames)));
+    if (method == 2)
+      generic::ensemble_nonlinear<2><<<grid, generic::kWarps * 32>>>(a);
+    else
+      generic::ensemble_nonlinear<3><<<grid, generic::kWarps * 32>>>(a);
+    return launch_status();
+  }
+  // The sort rewrites keys, values and the bounding box (cleared inside) on every call.
+  a.order = voxel_order(scan, nv, scratch, kStaticScratchBytes);
+  const size_t ntiles = (nv + das::kTileVoxels - 1) / das::kTileVoxels;
+  rcabeam_status st = method == 0   ? run_staged<false, das::kOpw>(a, ntiles)
+                      : method == 5 ? run_staged<false, das::kApertures>(a, ntiles)
+                                    : run_staged<false, das::kXdoppler>(a, ntiles);
+  if (st != RCABEAM_SUCCESS) return st;
+  if (method == 1) {
+    das::finish_magnitude<<<unsigned((nv + 255) / 256), 256>>>(pd, nv);
+    return launch_status();
+  }
+  return RCABEAM_SUCCESS;
+}
+
 }  // namespace rcb
 
 using namespace rcb;
@@ -554,6 +642,14 @@ rcabeam_status rcabeam_ensemble_workspace_bytes(size_t nv, size_t nc, size_t na,
   size_t documented = 2 * nv * (nc + na) * 16;
   *bytes = need ? (need < documented ? need : documented) : 256;
   return RCABEAM_SUCCESS;
+}
+
+rcabeam_status rcabeam_ensemble_static_device(const void* rc, const void* cr, const float* scan, const float* xe,
+                                              const float* ye, const float* angles, const float* starts, float* pd,
+                                              void* signal, size_t ns, size_t nc, size_t na, size_t nt, size_t nv,
+                                              float c, float fs, float fd, float fn, int method) {
+  return ensemble_static(rc, cr, scan, xe, ye, angles, starts, pd, signal, ns, nc, na, nt, nv, c, fs, fd, fn,
+                         method);
 }
 
 rcabeam_status rcabeam_device_error(int* code) {
