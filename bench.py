@@ -42,6 +42,12 @@ PITCH = 0.11e-3
 FS, FD, C = 20e6, 15e6, 1540.0
 T_START = 4e-6
 RANK_START = 3
+# DRAM bytes (read + write) per unit of the bf16x3 tensor-core DAS launch,
+# from one ncu capture: 1012.2 MB for 65,536 voxels x 256 ch x 11 ang x 104 frm.
+DAS_DRAM_BYTES_PER_UNIT = 1012.19e6 / (65536 * 256 * 11 * 104)
+
+
+SUBGRID = None  # (nx, nz, ny) central block of the full grid, same spacing (profiling)
 
 
 def workload():
@@ -51,11 +57,13 @@ def workload():
     half = (NC - 1) / 2 * PITCH
     grid = (np.linspace(-half, half, GRID_SHAPE[0]), np.linspace(4e-3, 12e-3, GRID_SHAPE[1]),
             np.linspace(-half, half, GRID_SHAPE[2]))
+    if SUBGRID:
+        grid = tuple(axis[(len(axis) - n) // 2:(len(axis) - n) // 2 + n] for axis, n in zip(grid, SUBGRID))
     return el, angles, grid
 
 
 def units_per_step() -> int:
-    return int(np.prod(GRID_SHAPE)) * 2 * NC * NA * NT
+    return int(np.prod(SUBGRID or GRID_SHAPE)) * 2 * NC * NA * NT
 
 
 CONFIG = {
@@ -228,12 +236,13 @@ def run_b200(args, rank: int, world: int) -> dict | None:
     # Tensor work of the dominant kernel: per (128-voxel tile, frame pass, aperture,
     # channel, angle) step, two 64-voxel groups x 3 products of one
     # M=128 x N=2*frames x K=16 MMA (sub-window splits excluded).
-    tiles = (int(np.prod(GRID_SHAPE)) + 127) // 128
+    tiles = (int(np.prod(SUBGRID or GRID_SHAPE)) + 127) // 128
     passes = (NT + 127) // 128
     frames = ((NT + passes - 1) // passes + 7) // 8 * 8
     mma_flops = tiles * passes * 2 * NC * NA * 2 * 3 * 2 * 128 * (2 * frames) * 16
     # Compulsory HBM bytes of one DAS launch: hi+lo packed planes read, IQ + power written.
-    das_bytes = 2 * NS * NC * NA * NT * 8 + int(np.prod(GRID_SHAPE)) * NT * 8 + int(np.prod(GRID_SHAPE)) * 8
+    nvox = int(np.prod(SUBGRID or GRID_SHAPE))
+    das_bytes = 2 * NS * NC * NA * NT * 8 + nvox * NT * 8 + nvox * 8
     tensor_peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops", 1590.0))
     line = {
         "metric": "OPW Gsamples/s (vox*ch*ang*frm), filtered PD", "value": ch["gsamples_per_s"],
@@ -246,7 +255,11 @@ def run_b200(args, rank: int, world: int) -> dict | None:
         "forms": results, "accuracy": accuracy, "e2e": e2e,
         "roofline": {"bound": "tensor", "kernel": "opw_tc<bf16x3> (DAS)",
                      "achieved": round(mma_flops / das_s / 1e12, 1), "peak": tensor_peak, "unit": "TFLOP/s",
-                     "frac": round(mma_flops / das_s / 1e12 / tensor_peak, 4), "traffic": None,
+                     "frac": round(mma_flops / das_s / 1e12 / tensor_peak, 4),
+                     "traffic": round(DAS_DRAM_BYTES_PER_UNIT * units),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one opw_tc launch on the "
+                                       "central 32x64x32 block (104 frames), scaled by units "
+                                       "(profiles/opw_tc_bf16x3_central_block_ncu.md)",
                      "das_ms": ch["das_ms"],
                      "note": "dense tcgen05 MMA flops issued per launch (2 groups x 3 products x M128 x N208 x K16 per "
                              "128-voxel tile step) vs "
@@ -336,8 +349,14 @@ def main() -> None:
                     help="reduced grid for profiling runs (the reported workload is the default)")
     ap.add_argument("--frames", type=int, default=None, help="reduced frame count for profiling runs")
     ap.add_argument("--channels", type=int, default=None, help="reduced channel count for profiling runs")
+    ap.add_argument("--subgrid", type=int, nargs=3, default=None, metavar=("NX", "NZ", "NY"),
+                    help="central block of the full grid at full resolution (profiling runs)")
     args = ap.parse_args()
-    global GRID_SHAPE, NT, NC
+    global GRID_SHAPE, NT, NC, SUBGRID
+    if args.subgrid:
+        SUBGRID = tuple(args.subgrid)
+        CONFIG["grid"] = list(SUBGRID)
+        CONFIG["workload"] += f" (REDUCED to the central {SUBGRID} block for profiling)"
     if args.channels:
         NC = args.channels
         CONFIG["channels"] = NC
