@@ -3,6 +3,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cub/device/device_radix_sort.cuh>
@@ -15,6 +16,7 @@
 #include "das_generic.cuh"
 #include "das_staged.cuh"
 #include "das_tc.cuh"
+#include "gram_tc.cuh"
 #include "pack.cuh"
 
 namespace rcb {
@@ -562,10 +564,58 @@ rcabeam_status rcabeam_clutter_scale_device(const void* iq, size_t n, int comple
   return launch_status();
 }
 
+// Tensor-core Gram (precision 2 = TF32, 3 = 3xBF16) of a complex64 Casorati
+// matrix: the rows x 2T float32 view as a 2-D tensor with 32 x 16 SWIZZLE_128B
+// boxes, one CTA per (unit, row slice).
+static rcabeam_status gram_tc_launch(const void* iq, size_t rows, size_t nt, const double* scale, bool tf32,
+                                     double* upper) {
+  auto fn = encode_fn();
+  if (!fn) return RCABEAM_ERROR_CUDA;
+  gramtc::Params prm{};
+  const int nb = int((2 * nt + gramtc::kBlock - 1) / gramtc::kBlock);
+  prm.nunits = gramtc::plan_units(nb, prm.units, &prm.nload_max);
+  if (!prm.nunits) return RCABEAM_ERROR_ARGUMENT;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  prm.slices = sms / prm.nunits > 0 ? sms / prm.nunits : 1;
+  const size_t per = (rows + prm.slices - 1) / prm.slices;
+  prm.slice_rows = (long long)((per + gramtc::kRows - 1) / gramtc::kRows * gramtc::kRows);
+  prm.slices = int((rows + prm.slice_rows - 1) / prm.slice_rows);
+  prm.rows = (long long)rows;
+  prm.nt = int(nt);
+  prm.scale = scale;
+  prm.upper = upper;
+  prm.err = device_error_ptr();
+  CUtensorMap map;
+  cuuint64_t dims[2] = {2 * nt, rows};
+  cuuint64_t strides[1] = {2 * nt * 4};
+  cuuint32_t box[2] = {32, cuuint32_t(gramtc::kRows)};
+  cuuint32_t estr[2] = {1, 1};
+  if (fn(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(iq), dims, strides, box, estr,
+         CU_TENSOR_MAP_INTERLEAVE_NONE, tf32 ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B : CU_TENSOR_MAP_SWIZZLE_128B,
+         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return RCABEAM_ERROR_ARGUMENT;
+  // At least 120 KB keeps one CTA (and one 512-column TMEM allocation) per SM.
+  const size_t smem = std::max(gramtc::smem_bytes(prm.nload_max), size_t(120) << 10);
+  auto kern = tf32 ? gramtc::gram_tc<true> : gramtc::gram_tc<false>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+    return RCABEAM_ERROR_CUDA;
+  kern<<<unsigned(prm.nunits * prm.slices), gramtc::kThreads, smem>>>(map, prm);
+  return launch_status();
+}
+
 rcabeam_status rcabeam_gram_accumulate_device(const void* iq, size_t rows, size_t nt, int complex128,
                                               const double* scale, int precision, double* upper) {
   if (!iq || !scale || !upper || !rows || !nt || nt > 65535) return RCABEAM_ERROR_ARGUMENT;
-  if (precision != 0 && precision != 1) return RCABEAM_ERROR_ARGUMENT;
+  if (precision < 0 || precision > 3) return RCABEAM_ERROR_ARGUMENT;
+  if (precision >= 2) {
+    // complex64 rows whose 8 nt-byte stride is a multiple of 16; T <= 1024; rows < 2^31.
+    if (complex128 || nt % 2 || nt > 1024 || rows >= (size_t(1) << 31) ||
+        reinterpret_cast<uintptr_t>(iq) % 16 != 0)
+      return RCABEAM_ERROR_ARGUMENT;
+    return gram_tc_launch(iq, rows, nt, scale, precision == 2, upper);
+  }
   int nb = int((nt + clutter::kGramTile - 1) / clutter::kGramTile);
   unsigned tiles = unsigned(nb * (nb + 1) / 2);
   size_t want = (148 * 8 + tiles - 1) / tiles;

@@ -28,6 +28,11 @@ import torch
 from rcabeam_b200 import _lib
 
 _GRAM_PRECISION = {"complex128": 0, "complex64": 1, "tf32": 2, "bf16x3": 3}
+# Machine epsilon of the Gram's products, for the negative-eigenvalue tolerance
+# 64 eps T max|lambda| (gpu_clutter.py:171 uses the eigenvalue dtype's eps):
+# float64, float32, TF32 (10-bit mantissa) and the 3xBF16 split (whose dropped
+# lo x lo term is about 2^-16 of a product).
+_GRAM_EPS = {"complex128": 2.0 ** -52, "complex64": 2.0 ** -23, "tf32": 2.0 ** -10, "bf16x3": 2.0 ** -16}
 
 
 def _inputs(iq) -> tuple[torch.Tensor, ...]:
@@ -84,6 +89,8 @@ class Gram:
     def accumulate(self, arrays, precision: str) -> int:
         """Scale, then Gram of every array into one shared matrix; returns total rows."""
         prec = _GRAM_PRECISION[precision]
+        if prec >= 2 and (any(a.dtype != torch.complex64 for a in arrays) or self.frames % 2 or self.frames > 1024):
+            raise ValueError(f"Precision {precision} requires complex64 IQ with an even frame count <= 1024")
         self.scale.zero_()
         self.upper.zero_()
         for a in arrays:
@@ -138,7 +145,7 @@ def temporal_basis(iq, *, method: str = "gram", precision: str = "complex128", t
     if info != 0:
         raise np.linalg.LinAlgError(f"cuSOLVER eigendecomposition failed (info={info})")
     lam = gram.eigenvalues
-    eps = np.finfo(np.float64).eps
+    eps = _GRAM_EPS[precision]
     tolerance = float(64 * eps * frames * lam.abs().max().item())
     minimum = float(lam[0].item())
     scale = float(gram.scale.item())

@@ -61,6 +61,12 @@ def test_argument_rejection_without_gpu(built_library):
     # FP16 with an odd (2-byte) pointer.
     assert lib.rcabeam_opw_fp16_device(ctypes.c_void_p(18), *([bogus] * 9), 4, 1, 1, 1, 1, 1540.0, 1.0, 0.0,
                                        -1.0) == 2
+    # Tensor-core Gram: complex128 input, odd frame count, T > 1024, unaligned rows, unknown precision.
+    assert lib.rcabeam_gram_accumulate_device(bogus, 8, 8, 1, bogus, 2, bogus) == 2
+    assert lib.rcabeam_gram_accumulate_device(bogus, 8, 7, 0, bogus, 3, bogus) == 2
+    assert lib.rcabeam_gram_accumulate_device(bogus, 8, 1026, 0, bogus, 2, bogus) == 2
+    assert lib.rcabeam_gram_accumulate_device(ctypes.c_void_p(24), 8, 8, 0, bogus, 3, bogus) == 2
+    assert lib.rcabeam_gram_accumulate_device(bogus, 8, 8, 0, bogus, 4, bogus) == 2
     size = ctypes.c_size_t(0)
     assert lib.rcabeam_ensemble_workspace_bytes(1000, 4, 2, ctypes.byref(size)) == 0
     assert 0 < size.value <= 2 * 1000 * 6 * 16
