@@ -68,6 +68,17 @@ constexpr int kAMatBytes = 128 * kRows * 2;  // 4096: one 128 x 16 16-bit matrix
 template <bool BF16X3>
 constexpr float kCoefScale = BF16X3 ? 1.0f : 1024.0f;
 enum Meta : int { kStep = 0, kTileEnd = 1, kFinish = 2 };
+// The tensor core's float32 accumulation rounds each update toward zero, which
+// shrinks a long sum by about 1.3e-8 per update (1.1e-4 of the amplitude after
+// the ~8400 updates of a full-size 3-product tile).  The MMA therefore flushes
+// the accumulators every kSegSteps steps; the epilogue adds the segment sums in
+// float32 round-to-nearest registers and per-CTA global scratch (kMaxCtas CTAs
+// x 2 groups x 64 voxels x kMaxFrames complex), which bounds the bias to the
+// updates of one segment.
+constexpr int kSegSteps = 512;
+constexpr int kMaxCtas = 160;
+constexpr size_t kPartialPerCta = size_t(2) * kGroupVox * kMaxFrames;  // float2 per CTA
+enum AccKind : int { kAccPartial = 0, kAccFinal = 1, kAccFinalEmpty = 2 };
 
 struct Args {
   const void* x_hi[2];  // per aperture (RC, CR): FP16 or BF16 hi planes, packed (c, a, s, 2 nt)
@@ -80,6 +91,7 @@ struct Args {
   const unsigned* order;
   float* pd;
   float2* signal;
+  float2* partial;  // kMaxCtas x kPartialPerCta segment sums
   int ns, nc, na, nt, nv;
   double c, fs, fd, fn;
   int frames;      // frames per pass (multiple of 8, <= 128)
@@ -230,6 +242,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(meta + kStages);
   int* counter = reinterpret_cast<int*>(tmem_slot + 1);  // next ring stage to claim
   int* item_steps = counter + 1;                         // steps staged for the current item
+  volatile int* acc_kind = item_steps + 1;               // AccKind of the pending flush
   double* angle_tab = reinterpret_cast<double*>(ctrl + 1024);
   double* tx_delay = angle_tab + 3 * p.na;                                   // [2][na][128]
   float2* tx_phase = reinterpret_cast<float2*>(tx_delay + 2 * p.na * kVox);  // [2][na][128]
@@ -240,7 +253,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&full[s], 32);  // the writing builder warp
       mbar_init(&empty[s], 1);  // tcgen05.commit (or a plain arrive for markers)
     }
-    mbar_init(acc_full, 1);
+    mbar_init(acc_full, 2);  // tcgen05.commit + the MMA thread's release of acc_kind
     mbar_init(acc_empty, 4);
     mbar_init(drain, 1);
     *counter = 0;
@@ -454,27 +467,33 @@ __global__ void __launch_bounds__(kThreads, 1)
     // ---------------------------------------------------------------- MMA --
     if (lane == 0) {
       const uint32_t idesc = instr_desc(BF16X3, 128, p.ncols);
-      uint32_t k = 0, tiles_done = 0;
-      bool started = false;  // the current item owns the accumulators
-      bool issued = false;   // the current item has issued an MMA
+      uint32_t k = 0, flushes = 0;
+      bool need_empty = false;  // a flush is outstanding: the epilogue must drain TMEM first
+      bool issued = false;      // MMAs issued since the last flush
+      int seg = 0;              // steps in the current segment
+      auto flush = [&](int kind) {
+        *acc_kind = kind;
+        mma_commit(acc_full);  // arrives once the segment's MMAs have completed
+        mbar_arrive(acc_full);
+        ++flushes;
+        need_empty = true;
+        issued = false;
+        seg = 0;
+      };
       for (;;) {
         const int s = k % kStages;
         if (!mbar_wait(&full[s], (k / kStages) & 1, p.err, kErrWaitFull)) break;
         const int m = meta[s];
         if (m == kFinish) break;
-        if (!started) {
-          // The previous item's epilogue must have drained the accumulators.
-          if (tiles_done > 0 && !mbar_wait(acc_empty, (tiles_done - 1) & 1, p.err, kErrWaitEmpty)) break;
-          started = true;
+        if (need_empty) {
+          if (!mbar_wait(acc_empty, (flushes - 1) & 1, p.err, kErrWaitEmpty)) break;
+          need_empty = false;
         }
         tc_fence_after();
         if (m == kTileEnd) {
-          mma_commit(acc_full);  // arrives once this item's MMAs have completed
+          flush(issued ? kAccFinal : kAccFinalEmpty);
           mbar_arrive(&empty[s]);
           ++k;
-          ++tiles_done;
-          started = false;
-          issued = false;
           continue;
         }
         const uint32_t st = smem_u32(stages + size_t(s) * stage_bytes);
@@ -494,6 +513,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         issued = true;
         mma_commit(&empty[s]);  // frees the stage once these MMAs have read it
         ++k;
+        if (++seg == kSegSteps) flush(kAccPartial);
       }
       // Every issued MMA has completed before the warp leaves (TMEM is freed after).
       mma_commit(drain);
@@ -505,40 +525,69 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int q = warp & 3;  // TMEM lane quarter this warp may access
     const int m = 32 * q + lane;
     const bool is_p = (m & 1) == 0;
-    uint32_t tiles_done = 0;
-    for (int item = blockIdx.x; item < work_items; item += gridDim.x) {
+    float2* part = p.partial + size_t(blockIdx.x) * kPartialPerCta;
+    uint32_t flushes = 0;
+    bool fail = false;
+    for (int item = blockIdx.x; item < work_items && !fail; item += gridDim.x) {
       const int tile = item / p.chunks, chunk = item % p.chunks;
-      if (!__all_sync(0xffffffffu, mbar_wait(acc_full, tiles_done & 1, p.err, kErrWaitFull))) break;
-      tc_fence_after();
       const int f0 = chunk * p.frames;
-      for (int g = 0; g < 2; ++g) {
-        const size_t qv = size_t(tile) * kVox + kGroupVox * g + (m >> 1);
-        const unsigned v = qv < size_t(p.nv) ? (p.order ? p.order[qv] : unsigned(qv)) : UINT_MAX;
-        float power = 0.f;
-        for (int c0 = 0; c0 < p.ncols; c0 += 32) {
-          float val[32];
-          tmem_ld32(tmem + (uint32_t(32 * q) << 16) + 256u * g + uint32_t(c0), val);
-          // The partner lane holds the other half (P <-> Q) of the same voxel.
+      for (int nflush = 0;; ++nflush) {
+        if (!__all_sync(0xffffffffu, mbar_wait(acc_full, flushes & 1, p.err, kErrWaitFull))) {
+          fail = true;
+          break;
+        }
+        const int kind = *acc_kind;
+        tc_fence_after();
+        const bool last = kind != kAccPartial;
+        for (int g = 0; g < 2; ++g) {
+          const int vg = m >> 1;  // voxel within the group
+          // Frame-major scratch: the even lanes of a warp touch 16 consecutive float2.
+          float2* pcol = part + size_t(g) * kMaxFrames * kGroupVox + vg;
+          const size_t qv = size_t(tile) * kVox + kGroupVox * g + vg;
+          const unsigned v = qv < size_t(p.nv) ? (p.order ? p.order[qv] : unsigned(qv)) : UINT_MAX;
+          float power = 0.f;
+          for (int c0 = 0; c0 < p.ncols; c0 += 32) {
+            float val[32];
+            if (kind != kAccFinalEmpty) {
+              tmem_ld32(tmem + (uint32_t(32 * q) << 16) + 256u * g + uint32_t(c0), val);
+            } else {
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            const float other_re = __shfl_xor_sync(0xffffffffu, val[2 * i], 1);
-            const float other_im = __shfl_xor_sync(0xffffffffu, val[2 * i + 1], 1);
-            // P lane: D = (P_re - Q_im, P_im + Q_re).
-            const float dre = (val[2 * i] - other_im) * (1.0f / kCoefScale<BF16X3>);
-            const float dim = (val[2 * i + 1] + other_re) * (1.0f / kCoefScale<BF16X3>);
-            const int frame = f0 + (c0 >> 1) + i;
-            if (is_p && v != UINT_MAX && frame < p.nt && frame < f0 + p.frames) {
-              if (p.signal) p.signal[size_t(v) * p.nt + frame] = make_float2(dre, dim);
-              power += dre * dre + dim * dim;
+              for (int i = 0; i < 32; ++i) val[i] = 0.f;
+            }
+            // Earlier segments' sums of these 16 frames (loads issued together).
+            float2 prev[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const int fl = (c0 >> 1) + i;
+              prev[i] = (nflush > 0 && is_p && fl < p.frames) ? pcol[size_t(fl) * kGroupVox] : make_float2(0.f, 0.f);
+            }
+            // The partner lane holds the other half (P <-> Q) of the same voxel.
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const float other_re = __shfl_xor_sync(0xffffffffu, val[2 * i], 1);
+              const float other_im = __shfl_xor_sync(0xffffffffu, val[2 * i + 1], 1);
+              const int fl = (c0 >> 1) + i;  // frame within the pass
+              if (is_p && fl < p.frames) {
+                // P lane: D = (P_re - Q_im, P_im + Q_re).
+                float2 acc = make_float2((val[2 * i] - other_im) * (1.0f / kCoefScale<BF16X3>) + prev[i].x,
+                                         (val[2 * i + 1] + other_re) * (1.0f / kCoefScale<BF16X3>) + prev[i].y);
+                if (!last) {
+                  pcol[size_t(fl) * kGroupVox] = acc;
+                } else if (v != UINT_MAX && f0 + fl < p.nt) {
+                  if (p.signal) p.signal[size_t(v) * p.nt + f0 + fl] = acc;
+                  power += acc.x * acc.x + acc.y * acc.y;
+                }
+              }
             }
           }
+          if (last && is_p && v != UINT_MAX) atomicAdd(p.pd + 2 * size_t(v), power / float(p.nt));
         }
-        if (is_p && v != UINT_MAX) atomicAdd(p.pd + 2 * size_t(v), power / float(p.nt));
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acc_empty);
+        ++flushes;
+        if (last) break;
       }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(acc_empty);
-      ++tiles_done;
     }
   }
   __syncthreads();

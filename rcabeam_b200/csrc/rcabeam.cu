@@ -258,6 +258,24 @@ static size_t tc_smem_bytes(bool bf16x3, size_t nt, size_t na) {
 }
 
 // Tensor-core OPW over all (tile, frame pass) work items with one persistent CTA per SM.
+// Segment sums of the tensor-core DAS (one slice per resident CTA; launches
+// are serialized on the default stream, so one buffer per device suffices).
+static __device__ float2 g_tc_partials[tc::kMaxCtas * tc::kPartialPerCta];
+
+static float2* tc_partials_address() {
+  static std::mutex lock;
+  static float2* addresses[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> guard(lock);
+  if (!addresses[dev]) {
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_tc_partials) != cudaSuccess) return nullptr;
+    addresses[dev] = static_cast<float2*>(ptr);
+  }
+  return addresses[dev];
+}
+
 template <bool BF16X3>
 static rcabeam_status run_tc(tc::Args a) {
   const size_t nt = size_t(a.nt);
@@ -286,8 +304,10 @@ static rcabeam_status run_tc(tc::Args a) {
   auto kern = tc::opw_tc<BF16X3>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
     return RCABEAM_ERROR_CUDA;
+  a.partial = tc_partials_address();
+  if (!a.partial) return RCABEAM_ERROR_CUDA;
   const int items = a.ntiles * a.chunks;
-  const unsigned grid = unsigned(items < sms ? items : sms);
+  const unsigned grid = unsigned(std::min(std::min(items, sms), tc::kMaxCtas));
   kern<<<grid, tc::kThreads, smem>>>(mh[0], mh[1], ml[0], ml[1], a);
   return launch_status();
 }
