@@ -224,6 +224,33 @@ rcabeam_status rcabeam_ensemble_static_device(const void* rc, const void* cr, co
                                               void* signal, size_t ns, size_t nc, size_t na, size_t nt, size_t nv,
                                               float c, float fs, float fd, float fn, int method);
 
+/* Differentiable OPW (extension; no counterpart in the reference interface).
+ * The OPW model of rcabeam_ensemble_device (method 0) with a per-receive-
+ * element delay offset offsets[A * nc + c] (seconds; A = 0 RC, 1 CR) added to
+ * every delay and a float64 sound speed c.  rc, cr: channels in the USER
+ * layout (ns, nc, na, nt), complex64 (complex128 = 0) or complex128.  voxels:
+ * nvl indices into scan (null: the first nvl voxels).  One call covers frames
+ * [frame0, frame0 + frames), frames <= 8.
+ * Forward: iq (nvl x frames, the channels' complex type) and/or power (nvl
+ * float64) += sum_t |IQ|^2 / nt. */
+rcabeam_status rcabeam_opw_offsets_forward_device(const void* rc, const void* cr, const float* scan,
+                                                  const unsigned* voxels, size_t nvl, const float* xe,
+                                                  const float* ye, const float* angles, const float* starts,
+                                                  const double* offsets, double c, float fs, float fd, float fn,
+                                                  size_t ns, size_t nc, size_t na, size_t nt, size_t frame0,
+                                                  size_t frames, void* iq, double* power, int complex128);
+
+/* Adjoint of the forward above for the upstream gradient grad_iq (nvl x frames,
+ * dL/dRe + j dL/dIm): adds to grad_rc / grad_cr (user layout, channels' type;
+ * atomics), grad_offsets (2 * nc float64) and *grad_c (float64). */
+rcabeam_status rcabeam_opw_offsets_adjoint_device(const void* rc, const void* cr, const float* scan,
+                                                  const unsigned* voxels, size_t nvl, const float* xe,
+                                                  const float* ye, const float* angles, const float* starts,
+                                                  const double* offsets, double c, float fs, float fd, float fn,
+                                                  size_t ns, size_t nc, size_t na, size_t nt, size_t frame0,
+                                                  size_t frames, const void* grad_iq, void* grad_rc, void* grad_cr,
+                                                  double* grad_offsets, double* grad_c, int complex128);
+
 /* Reads and clears the device error word set by a kernel whose bounded wait
  * gave up (0 = no error).  Synchronizes the device. */
 rcabeam_status rcabeam_device_error(int* code);

@@ -7,7 +7,7 @@ when the library has not been built: there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes
-from ctypes import c_float, c_int, c_size_t, c_void_p
+from ctypes import c_double, c_float, c_int, c_size_t, c_void_p
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "lib" / "librcabeam.so"
@@ -16,6 +16,7 @@ P = c_void_p
 Z = c_size_t
 F = c_float
 I = c_int
+D = c_double
 
 # name -> argument types (every function returns rcabeam_status, an int enum).
 SIGNATURES: dict[str, list] = {
@@ -43,6 +44,9 @@ SIGNATURES: dict[str, list] = {
     "rcabeam_project_device": [P, P, P, Z, Z, I, P, Z, I],
     "rcabeam_ensemble_static_device": [P, P, P, P, P, P, P, P, P, Z, Z, Z, Z, Z, F, F, F, F, I],
     "rcabeam_ensemble_workspace_bytes": [Z, Z, Z, ctypes.POINTER(c_size_t)],
+    "rcabeam_opw_offsets_forward_device": [P, P, P, P, Z, P, P, P, P, P, D, F, F, F, Z, Z, Z, Z, Z, Z, P, P, I],
+    "rcabeam_opw_offsets_adjoint_device": [P, P, P, P, Z, P, P, P, P, P, D, F, F, F, Z, Z, Z, Z, Z, Z, P, P, P, P, P,
+                                           I],
     "rcabeam_device_error": [ctypes.POINTER(c_int)],
 }
 

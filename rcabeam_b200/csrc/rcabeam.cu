@@ -13,6 +13,7 @@
 
 #include "clutter.cuh"
 #include "common.cuh"
+#include "das_adjoint.cuh"
 #include "das_generic.cuh"
 #include "das_staged.cuh"
 #include "das_tc.cuh"
@@ -965,3 +966,80 @@ rcabeam_status rcabeam_dmas_ccf_acf_from_channels_device(const void* iq_rc, cons
 }
 
 }  // extern "C"
+
+// ------------------------------------------------- differentiable OPW --
+static bool adjoint_geometry(adj::Geometry* g, const float* scan, const unsigned* voxels, size_t nvl,
+                             const float* xe, const float* ye, const float* angles, const float* starts,
+                             const double* offsets, double c, float fs, float fd, float fn, size_t ns, size_t nc,
+                             size_t na, size_t nt, size_t frame0, size_t frames) {
+  if (!scan || !xe || !ye || !angles || !starts || !offsets || !nvl || ns < 2 || !nc || !na || !nt || !frames ||
+      frames > size_t(adj::kChunk) || frame0 + frames > nt || !(c > 0) || !(fs > 0) || !std::isfinite(c) ||
+      !std::isfinite(fs) || !std::isfinite(fd) || !std::isfinite(fn) || nvl > INT32_MAX || ns > INT32_MAX ||
+      nc > 65535 || na > 65535 || nt > INT32_MAX)
+    return false;
+  g->scan = scan;
+  g->voxels = voxels;
+  g->xe = xe;
+  g->ye = ye;
+  g->angles = angles;
+  g->starts = starts;
+  g->offsets = offsets;
+  g->c = c;
+  g->fs = fs;
+  g->fd = fd;
+  g->fn = fn;
+  g->nvl = int(nvl);
+  g->ns = int(ns);
+  g->nc = int(nc);
+  g->na = int(na);
+  g->nt = int(nt);
+  g->f0 = int(frame0);
+  g->frames = int(frames);
+  return true;
+}
+
+rcabeam_status rcabeam_opw_offsets_forward_device(const void* rc, const void* cr, const float* scan,
+                                                  const unsigned* voxels, size_t nvl, const float* xe,
+                                                  const float* ye, const float* angles, const float* starts,
+                                                  const double* offsets, double c, float fs, float fd, float fn,
+                                                  size_t ns, size_t nc, size_t na, size_t nt, size_t frame0,
+                                                  size_t frames, void* iq, double* power, int complex128) {
+  adj::Geometry g;
+  if (!rc || !cr || (!iq && !power) ||
+      !adjoint_geometry(&g, scan, voxels, nvl, xe, ye, angles, starts, offsets, c, fs, fd, fn, ns, nc, na, nt, frame0,
+                        frames))
+    return RCABEAM_ERROR_ARGUMENT;
+  const unsigned blocks = unsigned((nvl + 127) / 128);
+  if (complex128)
+    adj::forward<double><<<blocks, 128>>>(g, static_cast<const double2*>(rc), static_cast<const double2*>(cr),
+                                          static_cast<double2*>(iq), power);
+  else
+    adj::forward<float><<<blocks, 128>>>(g, static_cast<const float2*>(rc), static_cast<const float2*>(cr),
+                                         static_cast<float2*>(iq), power);
+  return launch_status();
+}
+
+rcabeam_status rcabeam_opw_offsets_adjoint_device(const void* rc, const void* cr, const float* scan,
+                                                  const unsigned* voxels, size_t nvl, const float* xe,
+                                                  const float* ye, const float* angles, const float* starts,
+                                                  const double* offsets, double c, float fs, float fd, float fn,
+                                                  size_t ns, size_t nc, size_t na, size_t nt, size_t frame0,
+                                                  size_t frames, const void* grad_iq, void* grad_rc, void* grad_cr,
+                                                  double* grad_offsets, double* grad_c, int complex128) {
+  adj::Geometry g;
+  if (!rc || !cr || !grad_iq || !grad_rc || !grad_cr || !grad_offsets || !grad_c ||
+      !adjoint_geometry(&g, scan, voxels, nvl, xe, ye, angles, starts, offsets, c, fs, fd, fn, ns, nc, na, nt, frame0,
+                        frames))
+    return RCABEAM_ERROR_ARGUMENT;
+  const size_t threads = nvl * 2 * nc;
+  const unsigned blocks = unsigned((threads + 127) / 128);
+  if (complex128)
+    adj::adjoint<double><<<blocks, 128>>>(g, static_cast<const double2*>(rc), static_cast<const double2*>(cr),
+                                          static_cast<const double2*>(grad_iq), static_cast<double2*>(grad_rc),
+                                          static_cast<double2*>(grad_cr), grad_offsets, grad_c);
+  else
+    adj::adjoint<float><<<blocks, 128>>>(g, static_cast<const float2*>(rc), static_cast<const float2*>(cr),
+                                         static_cast<const float2*>(grad_iq), static_cast<float2*>(grad_rc),
+                                         static_cast<float2*>(grad_cr), grad_offsets, grad_c);
+  return launch_status();
+}
