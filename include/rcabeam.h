@@ -8,9 +8,11 @@
  * device error word of the bounded-wait kernels.
  *
  * All pointers are device pointers unless stated otherwise.  Work is launched
- * on the legacy default CUDA stream, as in the reference (rcabeam.h:200), and
- * calls return once the work is enqueued.  Nothing here allocates device
- * memory except the clutter-filter extensions, which say so.
+ * on the legacy default CUDA stream, as in the reference (rcabeam.h:200),
+ * except rcabeam_batch_run_device, which takes a stream so that it can be
+ * captured into a CUDA graph; calls return once the work is enqueued.  Nothing
+ * here allocates device memory except the clutter-filter extensions, which say
+ * so (the library's fixed scratch arrays are static device memory).
  */
 #pragma once
 
@@ -250,6 +252,53 @@ rcabeam_status rcabeam_opw_offsets_adjoint_device(const void* rc, const void* cr
                                                   size_t ns, size_t nc, size_t na, size_t nt, size_t frame0,
                                                   size_t frames, const void* grad_iq, void* grad_rc, void* grad_cr,
                                                   double* grad_offsets, double* grad_c, int complex128);
+
+/* Batch queue (extension; no counterpart in the reference interface): a queue
+ * of uneven ensembles reconstructed by one persistent kernel.  Each entry
+ * describes one ensemble with packed (c, a, s, t) complex64 channels and its
+ * own grid (scan, optional traversal order from rcabeam_voxel_order_device),
+ * geometry, power output (2 * nv floats, result in the even entries) and
+ * method: 0 OPW, 1 XDoppler, 3 DMAS-CCF-ACF.  frames_per_chunk (16, 32, 64;
+ * 0 = 64) is the staged methods' frame chunk, chosen by an autotuner. */
+typedef struct rcabeam_batch_ensemble {
+  const void* rc;
+  const void* cr;
+  const float* scan;
+  const unsigned* order;
+  const float* xe;
+  const float* ye;
+  const float* angles;
+  const float* starts;
+  float* pd;
+  size_t ns, nc, na, nt, nv;
+  float c, fs, fd, fn;
+  int method;
+  int frames_per_chunk;
+} rcabeam_batch_ensemble;
+
+/* Device table bytes of a queue of n ensembles (angles <= 64 per ensemble). */
+rcabeam_status rcabeam_batch_table_bytes(size_t n, const rcabeam_batch_ensemble* list, size_t* bytes);
+
+/* Writes the queue's device table (256-byte aligned; synchronous copies): call
+ * once per queue, before any stream capture of rcabeam_batch_run_device. */
+rcabeam_status rcabeam_batch_prepare(size_t n, const rcabeam_batch_ensemble* list, void* table,
+                                     size_t table_bytes);
+
+/* Enqueues on `stream` (a cudaStream_t; capturable into a CUDA graph): clears
+ * the counters and every pd, then runs the persistent kernel with ctas_per_sm
+ * (1-4) CTAs per SM.  times (device, n + 1 uint64): kernel start, then each
+ * ensemble's completion, in global-timer nanoseconds. */
+rcabeam_status rcabeam_batch_run_device(size_t n, const rcabeam_batch_ensemble* list, void* table,
+                                        size_t table_bytes, unsigned long long* times, int ctas_per_sm,
+                                        void* stream);
+
+/* Workspace bytes of rcabeam_voxel_order_device for nv voxels (128 <= nv < 2^31). */
+rcabeam_status rcabeam_voxel_order_workspace_bytes(size_t nv, size_t* bytes);
+
+/* Spatially compact traversal order (Morton codes of the voxel positions,
+ * radix-sorted) of nv voxels into order (nv unsigned), on the default stream. */
+rcabeam_status rcabeam_voxel_order_device(const float* scan, size_t nv, unsigned* order, void* workspace,
+                                          size_t workspace_bytes);
 
 /* Reads and clears the device error word set by a kernel whose bounded wait
  * gave up (0 = no error).  Synchronizes the device. */

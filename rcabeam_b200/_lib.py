@@ -47,6 +47,11 @@ SIGNATURES: dict[str, list] = {
     "rcabeam_opw_offsets_forward_device": [P, P, P, P, Z, P, P, P, P, P, D, F, F, F, Z, Z, Z, Z, Z, Z, P, P, I],
     "rcabeam_opw_offsets_adjoint_device": [P, P, P, P, Z, P, P, P, P, P, D, F, F, F, Z, Z, Z, Z, Z, Z, P, P, P, P, P,
                                            I],
+    "rcabeam_batch_table_bytes": [Z, P, ctypes.POINTER(c_size_t)],
+    "rcabeam_batch_prepare": [Z, P, P, Z],
+    "rcabeam_batch_run_device": [Z, P, P, Z, P, I, P],
+    "rcabeam_voxel_order_workspace_bytes": [Z, ctypes.POINTER(c_size_t)],
+    "rcabeam_voxel_order_device": [P, Z, P, P, Z],
     "rcabeam_device_error": [ctypes.POINTER(c_int)],
 }
 

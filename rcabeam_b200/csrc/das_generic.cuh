@@ -45,12 +45,11 @@ __device__ __forceinline__ float2 packed_sample(const float2* iq, const Tap& t, 
   return cmul(val, t.phase);
 }
 
+// One warp: voxel v (its row in scan / pd / signal), frames [128 fblock, 128 fblock + 128).
 template <int METHOD>
-__global__ void __launch_bounds__(kWarps * 32) ensemble_nonlinear(das::Args p) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const size_t v = size_t(blockIdx.x) * kWarps + warp;
-  if (v >= size_t(p.nv)) return;
-  const int fbase = blockIdx.y * 32 * kRegFrames + lane;
+__device__ void nonlinear_voxel(const das::Args& p, size_t v, int fblock) {
+  const int lane = threadIdx.x & 31;
+  const int fbase = fblock * 32 * kRegFrames + lane;
   const Voxel q = load_voxel(p.scan, v);
   const float2* rc = static_cast<const float2*>(p.rc);
   const float2* cr = static_cast<const float2*>(p.cr);
@@ -154,6 +153,13 @@ __global__ void __launch_bounds__(kWarps * 32) ensemble_nonlinear(das::Args p) {
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) total += __shfl_xor_sync(0xffffffffu, total, off);
   if (lane == 0) atomicAdd(p.pd + 2 * v, total / float(p.nt));
+}
+
+template <int METHOD>
+__global__ void __launch_bounds__(kWarps * 32) ensemble_nonlinear(das::Args p) {
+  const size_t v = size_t(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (v >= size_t(p.nv)) return;
+  nonlinear_voxel<METHOD>(p, v, blockIdx.y);
 }
 
 // --------------------------------------------- single-frame API (core.cu) --

@@ -88,32 +88,19 @@ __device__ __forceinline__ float4 load_pair(const unsigned char* p) {
   }
 }
 
-template <int LPV, bool HALF, int MODE, bool TMA>
-__global__ void __launch_bounds__(kThreads)
-    opw_staged(const __grid_constant__ CUtensorMap map_rc, const __grid_constant__ CUtensorMap map_cr, Args p) {
-  using S = Shape<LPV, HALF>;
-  constexpr bool kTwo = MODE != kOpw;
-  extern __shared__ __align__(1024) unsigned char smem[];
-  unsigned char* stage_data = smem;
-  StageTap* taps = reinterpret_cast<StageTap*>(smem + S::kOffTaps);
-  int* meta = reinterpret_cast<int*>(smem + S::kOffMeta);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S::kOffFull);
-  uint64_t* empty = reinterpret_cast<uint64_t*>(smem + S::kOffEmpty);
-  unsigned* vox = reinterpret_cast<unsigned*>(smem + S::kOffVox);
-  double* angle_tab = reinterpret_cast<double*>(smem + S::kOffAngles);
+// Shared-memory ring of one CTA: kStages slots of staged sample windows, the
+// voxel taps of every slot, a slot tag and the full / empty barriers.
+struct Ring {
+  unsigned char* data;
+  size_t slot_bytes;
+  StageTap* taps;  // [kStages][kTileVoxels]
+  int* meta;       // [kStages]: aperture of the slot, or kMetaEnd
+  uint64_t* full;
+  uint64_t* empty;
+};
 
-  const int warp = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
-  const int frame0 = p.frame_base + blockIdx.y * S::kFrames;
-  const size_t tile0 = size_t(blockIdx.x) * kTileVoxels;
-
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full[s], 32);
-      mbar_init(&empty[s], kConsumerWarps);
-    }
-    fence_mbar_init();
-  }
+// Voxel ids of one 64-voxel tile and the per-angle (cos, sin, start) table.
+__device__ __forceinline__ void load_item_tables(const Args& p, size_t tile0, unsigned* vox, double* angle_tab) {
   for (int i = threadIdx.x; i < kTileVoxels; i += blockDim.x) {
     size_t q = tile0 + i;
     vox[i] = q < size_t(p.nv) ? (p.order ? p.order[q] : unsigned(q)) : UINT_MAX;
@@ -124,124 +111,133 @@ __global__ void __launch_bounds__(kThreads)
     angle_tab[3 * a + 1] = sin(th);
     angle_tab[3 * a + 2] = double(p.starts[a]);
   }
-  __syncthreads();
+}
 
-  if (warp == kConsumerWarps) {
-    // ------------------------------------------------------------ producer --
-    if constexpr (TMA) {
-      if (lane == 0) {
-        prefetch_tensormap(&map_rc);
-        prefetch_tensormap(&map_cr);
-      }
-    }
-    double px[2], pz[2], py[2];
-    bool pv[2];
+// Producer warp of one (tile, frame chunk): stages every (aperture, channel,
+// angle) window, then a kMetaEnd slot.  k is the ring position (in/out).
+template <int LPV, bool HALF, bool TMA>
+__device__ bool produce_item(const CUtensorMap* map_rc, const CUtensorMap* map_cr, const Args& p,
+                             const unsigned* vox, const double* angle_tab, const Ring& ring, int frame0,
+                             uint32_t& k) {
+  using S = Shape<LPV, HALF>;
+  const int lane = threadIdx.x & 31;
+  double px[2], pz[2], py[2];
+  bool pv[2];
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      unsigned v = vox[lane + 32 * j];
-      pv[j] = v != UINT_MAX;
-      size_t b = pv[j] ? 3 * size_t(v) : 0;
-      px[j] = pv[j] ? double(p.scan[b]) : 0.0;
-      pz[j] = pv[j] ? double(p.scan[b + 1]) : 0.0;
-      py[j] = pv[j] ? double(p.scan[b + 2]) : 0.0;
-    }
-    uint32_t k = 0;
-    bool ok = true;
-    for (int config = 0; config < 2 && ok; ++config) {
-      const float* el = config ? p.ye : p.xe;
-      const CUtensorMap* map = config ? &map_cr : &map_rc;
-      const unsigned char* gsrc = static_cast<const unsigned char*>(config ? p.cr : p.rc);
-      for (int ch = 0; ch < p.nc && ok; ++ch) {
-        double e = double(el[ch]);
-        double trx[2];
-        bool act[2];
+  for (int j = 0; j < 2; ++j) {
+    unsigned v = vox[lane + 32 * j];
+    pv[j] = v != UINT_MAX;
+    size_t b = pv[j] ? 3 * size_t(v) : 0;
+    px[j] = pv[j] ? double(p.scan[b]) : 0.0;
+    pz[j] = pv[j] ? double(p.scan[b + 1]) : 0.0;
+    py[j] = pv[j] ? double(p.scan[b + 2]) : 0.0;
+  }
+  bool ok = true;
+  for (int config = 0; config < 2 && ok; ++config) {
+    const float* el = config ? p.ye : p.xe;
+    const CUtensorMap* map = config ? map_cr : map_rc;
+    const unsigned char* gsrc = static_cast<const unsigned char*>(config ? p.cr : p.rc);
+    for (int ch = 0; ch < p.nc && ok; ++ch) {
+      double e = double(el[ch]);
+      double trx[2];
+      bool act[2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        trx[j] = receive_delay(config ? py[j] : px[j], pz[j], e, p.c, p.fn, &act[j]);
+        act[j] = act[j] && pv[j];
+      }
+      for (int a = 0; a < p.na && ok; ++a) {
+        const double cs = angle_tab[3 * a], sn = angle_tab[3 * a + 1], st = angle_tab[3 * a + 2];
+        Tap t[2];
+        int lo = INT_MAX, hi = INT_MIN;
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-          trx[j] = receive_delay(config ? py[j] : px[j], pz[j], e, p.c, p.fn, &act[j]);
-          act[j] = act[j] && pv[j];
+          double ttx = transmit_delay(config ? px[j] : py[j], pz[j], cs, sn, p.c);
+          t[j] = make_tap(__dadd_rn(ttx, trx[j]), st, p.fs, p.fd, p.ns, act[j]);
+          if (t[j].i0 >= 0) {
+            lo = min(lo, t[j].i0);
+            hi = max(hi, t[j].i0);
+          }
         }
-        for (int a = 0; a < p.na && ok; ++a) {
-          const double cs = angle_tab[3 * a], sn = angle_tab[3 * a + 1], st = angle_tab[3 * a + 2];
-          Tap t[2];
-          int lo = INT_MAX, hi = INT_MIN;
+        lo = __reduce_min_sync(0xffffffffu, lo);
+        hi = __reduce_max_sync(0xffffffffu, hi);
+        if (lo == INT_MAX) continue;  // no voxel of the tile sees this slab
+        const int slab = ch * p.na + a;
+        for (int base = lo; base <= hi; base += kRows - 1) {
+          const int s = k % kStages;
+          ok = __all_sync(0xffffffffu, mbar_wait(&ring.empty[s], ((k / kStages) & 1) ^ 1, p.err, kErrWaitEmpty));
+          if (!ok) break;
 #pragma unroll
           for (int j = 0; j < 2; ++j) {
-            double ttx = transmit_delay(config ? px[j] : py[j], pz[j], cs, sn, p.c);
-            t[j] = make_tap(__dadd_rn(ttx, trx[j]), st, p.fs, p.fd, p.ns, act[j]);
-            if (t[j].i0 >= 0) {
-              lo = min(lo, t[j].i0);
-              hi = max(hi, t[j].i0);
-            }
+            int r = t[j].i0 - base;
+            bool in = t[j].i0 >= 0 && r >= 0 && r < kRows - 1;
+            StageTap q;
+            q.row = in ? r : -1;
+            q.w = t[j].w;
+            q.pr = t[j].phase.x;
+            q.pi = t[j].phase.y;
+            ring.taps[s * kTileVoxels + lane + 32 * j] = q;
           }
-          lo = __reduce_min_sync(0xffffffffu, lo);
-          hi = __reduce_max_sync(0xffffffffu, hi);
-          if (lo == INT_MAX) continue;  // no voxel of the tile sees this slab
-          const int slab = ch * p.na + a;
-          for (int base = lo; base <= hi; base += kRows - 1) {
-            const int s = k % kStages;
-            ok = __all_sync(0xffffffffu, mbar_wait(&empty[s], ((k / kStages) & 1) ^ 1, p.err, kErrWaitEmpty));
-            if (!ok) break;
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-              int r = t[j].i0 - base;
-              bool in = t[j].i0 >= 0 && r >= 0 && r < kRows - 1;
-              StageTap q;
-              q.row = in ? r : -1;
-              q.w = t[j].w;
-              q.pr = t[j].phase.x;
-              q.pi = t[j].phase.y;
-              taps[s * kTileVoxels + lane + 32 * j] = q;
-            }
-            if (lane == 0) meta[s] = config;
-            unsigned char* dst = stage_data + size_t(s) * S::kStageBytes;
-            if constexpr (TMA) {
-              __syncwarp();
-              if (lane == 0) {
-                mbar_arrive_expect_tx(&full[s], S::kStageBytes);
-                tma_load_3d(dst, map, &full[s], frame0, base, slab);
-              } else {
-                mbar_arrive(&full[s]);
-              }
+          if (lane == 0) ring.meta[s] = config;
+          unsigned char* dst = ring.data + size_t(s) * ring.slot_bytes;
+          if constexpr (TMA) {
+            __syncwarp();
+            if (lane == 0) {
+              mbar_arrive_expect_tx(&ring.full[s], S::kStageBytes);
+              tma_load_3d(dst, map, &ring.full[s], frame0, base, slab);
             } else {
-              // Plain staging: zero outside the slab, like the TMA out-of-bounds fill.
-              const size_t slab_off = size_t(slab) * p.ns;
-              for (int i = lane; i < kRows * S::kFrames; i += 32) {
-                int r = i / S::kFrames, f = i % S::kFrames;
-                int row = base + r, frame = frame0 + f;
-                bool inside = row < p.ns && frame < p.nt;
-                size_t g = ((slab_off + size_t(inside ? row : 0)) * p.nt + size_t(inside ? frame : 0)) * S::kElem;
-                if constexpr (HALF) {
-                  unsigned v = inside ? *reinterpret_cast<const unsigned*>(gsrc + g) : 0u;
-                  *reinterpret_cast<unsigned*>(dst + size_t(i) * 4) = v;
-                } else {
-                  float2 v = inside ? *reinterpret_cast<const float2*>(gsrc + g) : make_float2(0.f, 0.f);
-                  *reinterpret_cast<float2*>(dst + size_t(i) * 8) = v;
-                }
-              }
-              __syncwarp();
-              mbar_arrive(&full[s]);
+              mbar_arrive(&ring.full[s]);
             }
-            ++k;
+          } else {
+            // Plain staging: zero outside the slab, like the TMA out-of-bounds fill.
+            const size_t slab_off = size_t(slab) * p.ns;
+            for (int i = lane; i < kRows * S::kFrames; i += 32) {
+              int r = i / S::kFrames, f = i % S::kFrames;
+              int row = base + r, frame = frame0 + f;
+              bool inside = row < p.ns && frame < p.nt;
+              size_t g = ((slab_off + size_t(inside ? row : 0)) * p.nt + size_t(inside ? frame : 0)) * S::kElem;
+              if constexpr (HALF) {
+                unsigned v = inside ? *reinterpret_cast<const unsigned*>(gsrc + g) : 0u;
+                *reinterpret_cast<unsigned*>(dst + size_t(i) * 4) = v;
+              } else {
+                float2 v = inside ? *reinterpret_cast<const float2*>(gsrc + g) : make_float2(0.f, 0.f);
+                *reinterpret_cast<float2*>(dst + size_t(i) * 8) = v;
+              }
+            }
+            __syncwarp();
+            mbar_arrive(&ring.full[s]);
           }
+          ++k;
         }
       }
     }
-    if (ok) {
-      const int s = k % kStages;
-      ok = __all_sync(0xffffffffu, mbar_wait(&empty[s], ((k / kStages) & 1) ^ 1, p.err, kErrWaitEmpty));
-      if (ok) {
-        if (lane == 0) meta[s] = kMetaEnd;
-        __syncwarp();
-        mbar_arrive(&full[s]);
-        ++k;
-      }
-    }
-    // Drain: every issued copy has landed before this warp may leave.
-    for (uint32_t u = k > kStages ? k - kStages : 0; u < k; ++u) mbar_wait(&full[u % kStages], (u / kStages) & 1, p.err, kErrWaitDrain);
-    return;
   }
+  if (ok) {
+    const int s = k % kStages;
+    ok = __all_sync(0xffffffffu, mbar_wait(&ring.empty[s], ((k / kStages) & 1) ^ 1, p.err, kErrWaitEmpty));
+    if (ok) {
+      if (lane == 0) ring.meta[s] = kMetaEnd;
+      __syncwarp();
+      mbar_arrive(&ring.full[s]);
+      ++k;
+    }
+  }
+  return ok;
+}
 
-  // ------------------------------------------------------------- consumers --
+// Every copy the producer issued has landed (before the warp may leave).
+__device__ __forceinline__ void drain_ring(const Ring& ring, uint32_t k, int* err) {
+  for (uint32_t u = k > kStages ? k - kStages : 0; u < k; ++u)
+    mbar_wait(&ring.full[u % kStages], (u / kStages) & 1, err, kErrWaitDrain);
+}
+
+// Consumer warps (warp index cw in [0, kConsumerWarps)) of one (tile, frame
+// chunk): accumulate until the kMetaEnd slot, then write IQ and power.
+template <int LPV, bool HALF, int MODE>
+__device__ bool consume_item(const Args& p, const unsigned* vox, const Ring& ring, int frame0, int cw, uint32_t& k) {
+  using S = Shape<LPV, HALF>;
+  constexpr bool kTwo = MODE != kOpw;
+  const int lane = threadIdx.x & 31;
   constexpr int kVpi = 32 / LPV;  // voxels per warp instruction
   constexpr int kJ = (kTileVoxels + kConsumerWarps * kVpi - 1) / (kConsumerWarps * kVpi);
   const int vs = lane / LPV;
@@ -256,17 +252,23 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
   bool ok = true;
-  for (uint32_t k = 0;; ++k) {
+  for (;; ++k) {
     const int s = k % kStages;
-    ok = __all_sync(0xffffffffu, mbar_wait(&full[s], (k / kStages) & 1, p.err, kErrWaitFull));
+    ok = __all_sync(0xffffffffu, mbar_wait(&ring.full[s], (k / kStages) & 1, p.err, kErrWaitFull));
     if (!ok) break;
-    const int m = meta[s];
-    if (m == kMetaEnd) break;
-    const unsigned char* data = stage_data + size_t(s) * S::kStageBytes + pl * 2 * S::kElem;
-    const float4* tp = reinterpret_cast<const float4*>(taps + s * kTileVoxels);
+    const int m = ring.meta[s];
+    if (m == kMetaEnd) {
+      // The end slot is consumed too (released so the ring position stays shared).
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&ring.empty[s]);
+      ++k;
+      break;
+    }
+    const unsigned char* data = ring.data + size_t(s) * ring.slot_bytes + pl * 2 * S::kElem;
+    const float4* tp = reinterpret_cast<const float4*>(ring.taps + s * kTileVoxels);
 #pragma unroll
     for (int j = 0; j < kJ; ++j) {
-      const int slot = (j * kConsumerWarps + warp) * kVpi + vs;
+      const int slot = (j * kConsumerWarps + cw) * kVpi + vs;
       if (slot < kTileVoxels) {
         float4 q = tp[slot];
         int row = __float_as_int(q.x);
@@ -289,14 +291,14 @@ __global__ void __launch_bounds__(kThreads)
       }
     }
     __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[s]);
+    if (lane == 0) mbar_arrive(&ring.empty[s]);
   }
-  if (!ok) return;
+  if (!ok) return false;
 
   const float inv_nt = 1.0f / float(p.nt);
 #pragma unroll
   for (int j = 0; j < kJ; ++j) {
-    const int slot = (j * kConsumerWarps + warp) * kVpi + vs;
+    const int slot = (j * kConsumerWarps + cw) * kVpi + vs;
     const unsigned v = slot < kTileVoxels ? vox[slot] : UINT_MAX;
     float pr = 0.f, pi = 0.f;
     if (v != UINT_MAX) {
@@ -331,6 +333,44 @@ __global__ void __launch_bounds__(kThreads)
         if constexpr (MODE == kXdoppler) atomicAdd(p.pd + 2 * size_t(v) + 1, pi * inv_nt);
       }
     }
+  }
+  return true;
+}
+
+template <int LPV, bool HALF, int MODE, bool TMA>
+__global__ void __launch_bounds__(kThreads)
+    opw_staged(const __grid_constant__ CUtensorMap map_rc, const __grid_constant__ CUtensorMap map_cr, Args p) {
+  using S = Shape<LPV, HALF>;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const Ring ring{smem, S::kStageBytes, reinterpret_cast<StageTap*>(smem + S::kOffTaps),
+                  reinterpret_cast<int*>(smem + S::kOffMeta), reinterpret_cast<uint64_t*>(smem + S::kOffFull),
+                  reinterpret_cast<uint64_t*>(smem + S::kOffEmpty)};
+  unsigned* vox = reinterpret_cast<unsigned*>(smem + S::kOffVox);
+  double* angle_tab = reinterpret_cast<double*>(smem + S::kOffAngles);
+  const int warp = threadIdx.x >> 5;
+  const int frame0 = p.frame_base + blockIdx.y * S::kFrames;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&ring.full[s], 32);
+      mbar_init(&ring.empty[s], kConsumerWarps);
+    }
+    fence_mbar_init();
+  }
+  load_item_tables(p, size_t(blockIdx.x) * kTileVoxels, vox, angle_tab);
+  __syncthreads();
+  uint32_t k = 0;
+  if (warp == kConsumerWarps) {
+    if constexpr (TMA) {
+      if ((threadIdx.x & 31) == 0) {
+        prefetch_tensormap(&map_rc);
+        prefetch_tensormap(&map_cr);
+      }
+    }
+    produce_item<LPV, HALF, TMA>(&map_rc, &map_cr, p, vox, angle_tab, ring, frame0, k);
+    drain_ring(ring, k, p.err);
+  } else {
+    consume_item<LPV, HALF, MODE>(p, vox, ring, frame0, warp, k);
   }
 }
 

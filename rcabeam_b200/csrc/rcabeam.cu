@@ -8,11 +8,13 @@
 #include <cstdint>
 #include <cub/device/device_radix_sort.cuh>
 #include <mutex>
+#include <vector>
 
 #include <cusolverDn.h>
 
 #include "clutter.cuh"
 #include "common.cuh"
+#include "batch.cuh"
 #include "das_adjoint.cuh"
 #include "das_generic.cuh"
 #include "das_staged.cuh"
@@ -1043,3 +1045,173 @@ rcabeam_status rcabeam_opw_offsets_adjoint_device(const void* rc, const void* cr
                                          static_cast<float2*>(grad_cr), grad_offsets, grad_c);
   return launch_status();
 }
+
+// ---------------------------------------------------------- batch queue --
+namespace {
+struct BatchLayout {
+  size_t ens, maps, next, done, tile_done, total;
+};
+
+bool batch_plan(size_t n, const rcabeam_batch_ensemble* list, std::vector<batch::Ensemble>* out, BatchLayout* L,
+                long long* total_items) {
+  if (!n || !list || n > (1u << 20)) return false;
+  long long items = 0, tiles_xd = 0;
+  if (out) out->resize(n);
+  for (size_t i = 0; i < n; ++i) {
+    const rcabeam_batch_ensemble& d = list[i];
+    if (!d.rc || !d.cr || !d.scan || !d.xe || !d.ye || !d.angles || !d.starts || !d.pd || d.ns < 2 || !d.nc ||
+        !d.na || !d.nt || !d.nv || d.na > size_t(batch::kMaxAngles) || d.nv > INT32_MAX || d.ns > INT32_MAX ||
+        d.nc > INT32_MAX || d.nt > INT32_MAX || !(d.c > 0) || !(d.fs > 0) || !std::isfinite(d.c) ||
+        !std::isfinite(d.fs) || !std::isfinite(d.fd) || !std::isfinite(d.fn))
+      return false;
+    if (d.method != 0 && d.method != 1 && d.method != 3) return false;
+    const int fpc = d.frames_per_chunk ? d.frames_per_chunk : 64;
+    if (fpc != 16 && fpc != 32 && fpc != 64) return false;
+    batch::Ensemble e{};
+    e.method = d.method;
+    e.lpv = fpc / 2;
+    if (d.method == 3) {
+      e.tiles = int((d.nv + batch::kDmasVoxels - 1) / batch::kDmasVoxels);
+      e.chunks = int((d.nt + 127) / 128);
+    } else {
+      e.tiles = int((d.nv + das::kTileVoxels - 1) / das::kTileVoxels);
+      e.chunks = int((d.nt + fpc - 1) / fpc);
+    }
+    e.tma = (d.nt * 8) % 16 == 0 && reinterpret_cast<uintptr_t>(d.rc) % 16 == 0 &&
+            reinterpret_cast<uintptr_t>(d.cr) % 16 == 0 && encode_fn() != nullptr;
+    e.first_item = items;
+    e.tile_base = tiles_xd;
+    items += (long long)e.tiles * e.chunks;
+    if (d.method == 1) tiles_xd += e.tiles;
+    das::Args& a = e.args;
+    a.rc = d.rc;
+    a.cr = d.cr;
+    a.scan = d.scan;
+    a.xe = d.xe;
+    a.ye = d.ye;
+    a.angles = d.angles;
+    a.starts = d.starts;
+    a.order = d.order;
+    a.pd = d.pd;
+    a.signal = nullptr;
+    a.ns = int(d.ns);
+    a.nc = int(d.nc);
+    a.na = int(d.na);
+    a.nt = int(d.nt);
+    a.nv = int(d.nv);
+    a.c = d.c;
+    a.fs = d.fs;
+    a.fd = d.fd;
+    a.fn = d.fn;
+    a.frame_base = 0;
+    a.err = device_error_ptr();
+    if (out) (*out)[i] = e;
+  }
+  L->ens = 0;
+  L->maps = align256(n * sizeof(batch::Ensemble));
+  L->next = L->maps + align256(2 * n * sizeof(CUtensorMap));
+  L->done = L->next + 256;
+  L->tile_done = L->done + align256(n * 4);
+  L->total = L->tile_done + align256(size_t(tiles_xd > 0 ? tiles_xd : 1) * 4);
+  *total_items = items;
+  return true;
+}
+
+batch::Queue batch_queue(void* table, size_t n, const BatchLayout& L, long long total, unsigned long long* times) {
+  unsigned char* t = static_cast<unsigned char*>(table);
+  batch::Queue q{};
+  q.ens = reinterpret_cast<const batch::Ensemble*>(t + L.ens);
+  q.maps = reinterpret_cast<const CUtensorMap*>(t + L.maps);
+  q.n = int(n);
+  q.total_items = total;
+  q.next = reinterpret_cast<unsigned long long*>(t + L.next);
+  q.done = reinterpret_cast<unsigned*>(t + L.done);
+  q.tile_done = reinterpret_cast<unsigned*>(t + L.tile_done);
+  q.times = times;
+  q.err = device_error_ptr();
+  return q;
+}
+}  // namespace
+
+extern "C" {
+
+rcabeam_status rcabeam_batch_table_bytes(size_t n, const rcabeam_batch_ensemble* list, size_t* bytes) {
+  BatchLayout L;
+  long long total = 0;
+  if (!bytes || !batch_plan(n, list, nullptr, &L, &total)) return RCABEAM_ERROR_ARGUMENT;
+  *bytes = L.total;
+  return RCABEAM_SUCCESS;
+}
+
+rcabeam_status rcabeam_batch_prepare(size_t n, const rcabeam_batch_ensemble* list, void* table,
+                                     size_t table_bytes) {
+  BatchLayout L;
+  long long total = 0;
+  std::vector<batch::Ensemble> ens;
+  if (!table || reinterpret_cast<uintptr_t>(table) % 256 != 0 || !batch_plan(n, list, &ens, &L, &total) ||
+      table_bytes < L.total)
+    return RCABEAM_ERROR_ARGUMENT;
+  std::vector<CUtensorMap> maps(2 * n);
+  for (size_t i = 0; i < n; ++i) {
+    batch::Ensemble& e = ens[i];
+    if (e.method == 3 || !e.tma) continue;
+    const int frames = 2 * e.lpv;
+    const size_t slabs = size_t(e.args.nc) * e.args.na;
+    if (!make_slab_map(&maps[2 * i], e.args.rc, 8, size_t(e.args.nt), size_t(e.args.ns), slabs, frames, das::kRows) ||
+        !make_slab_map(&maps[2 * i + 1], e.args.cr, 8, size_t(e.args.nt), size_t(e.args.ns), slabs, frames,
+                       das::kRows))
+      e.tma = 0;
+  }
+  unsigned char* t = static_cast<unsigned char*>(table);
+  if (cudaMemcpy(t + L.ens, ens.data(), n * sizeof(batch::Ensemble), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(t + L.maps, maps.data(), 2 * n * sizeof(CUtensorMap), cudaMemcpyHostToDevice) != cudaSuccess)
+    return RCABEAM_ERROR_CUDA;
+  return RCABEAM_SUCCESS;
+}
+
+rcabeam_status rcabeam_batch_run_device(size_t n, const rcabeam_batch_ensemble* list, void* table,
+                                        size_t table_bytes, unsigned long long* times, int ctas_per_sm,
+                                        void* stream) {
+  BatchLayout L;
+  long long total = 0;
+  if (!table || !times || ctas_per_sm < 1 || ctas_per_sm > 3 || !batch_plan(n, list, nullptr, &L, &total) ||
+      table_bytes < L.total)
+    return RCABEAM_ERROR_ARGUMENT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  unsigned char* t = static_cast<unsigned char*>(table);
+  // Counters, completion times (start slot = all ones for the atomicMin) and every power map.
+  if (cudaMemsetAsync(t + L.next, 0, L.total - L.next, st) != cudaSuccess ||
+      cudaMemsetAsync(times, 0xff, 8, st) != cudaSuccess || cudaMemsetAsync(times + 1, 0, 8 * n, st) != cudaSuccess)
+    return RCABEAM_ERROR_CUDA;
+  for (size_t i = 0; i < n; ++i)
+    if (cudaMemsetAsync(list[i].pd, 0, 2 * list[i].nv * sizeof(float), st) != cudaSuccess) return RCABEAM_ERROR_CUDA;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  auto kern = ctas_per_sm == 1 ? batch::run<1> : ctas_per_sm == 2 ? batch::run<2> : batch::run<3>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(batch::Smem::kBytes)) !=
+      cudaSuccess)
+    return RCABEAM_ERROR_CUDA;
+  const long long want = (long long)sms * ctas_per_sm;
+  const unsigned grid = unsigned(total < want ? total : want);
+  kern<<<grid, das::kThreads, batch::Smem::kBytes, st>>>(batch_queue(table, n, L, total, times));
+  return cudaGetLastError() == cudaSuccess ? RCABEAM_SUCCESS : RCABEAM_ERROR_CUDA;
+}
+
+rcabeam_status rcabeam_voxel_order_workspace_bytes(size_t nv, size_t* bytes) {
+  if (!bytes) return RCABEAM_ERROR_ARGUMENT;
+  *bytes = order_bytes(nv, nullptr);
+  return *bytes ? RCABEAM_SUCCESS : RCABEAM_ERROR_ARGUMENT;
+}
+
+rcabeam_status rcabeam_voxel_order_device(const float* scan, size_t nv, unsigned* order, void* workspace,
+                                          size_t workspace_bytes) {
+  if (!scan || !order || !nv || !workspace) return RCABEAM_ERROR_ARGUMENT;
+  const unsigned* sorted = voxel_order(scan, nv, workspace, workspace_bytes);
+  if (!sorted) return RCABEAM_ERROR_ARGUMENT;
+  return cudaMemcpyAsync(order, sorted, nv * sizeof(unsigned), cudaMemcpyDeviceToDevice, 0) == cudaSuccess
+             ? RCABEAM_SUCCESS
+             : RCABEAM_ERROR_CUDA;
+}
+
+}  // extern "C"
