@@ -273,6 +273,89 @@ def run_b200(args, rank: int, world: int) -> dict | None:
     return line
 
 
+# --------------------------------------------------- batching form (queue) --
+def run_batching(args) -> dict:
+    """48 uneven ensembles (depth, frames, angles, method drawn from a seed) through the
+    persistent queue kernel under a CUDA graph, next to sequential plain launches."""
+    import torch
+
+    from rcabeam_b200 import _lib, batching
+    from rcabeam_b200.sim import RCAGeometry
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(args.seed)
+    n = args.ensembles
+    methods = ["opw"] * (n // 2) + ["xdoppler"] * (n // 4) + ["dmas"] * (n - n // 2 - n // 4)
+    methods = [methods[i] for i in rng.permutation(n)]
+    ns, nc = 512, 128
+    el = (np.arange(nc) - (nc - 1) / 2) * PITCH
+    half = (nc - 1) / 2 * PITCH
+    geom = RCAGeometry(el, el, c=C, fs=FS, f_demod=FD, fnumber=None)
+    dz = 8e-3 / 255
+    gen = torch.Generator(device=dev).manual_seed(args.seed)
+    ens, shapes = [], []
+    for i in range(n):
+        depth = int(rng.choice([128, 192, 256, 384]))
+        nt = int(rng.choice([50, 100, 200, 400]))
+        na = int(rng.choice([5, 7, 11]))
+        chans = [torch.randn((ns * nc * na * nt,), dtype=torch.complex64, generator=gen, device=dev)
+                 for _ in range(2)]
+        grid = (np.linspace(-half, half, 128), 4e-3 + dz * np.arange(depth), np.linspace(-half, half, 128))
+        e = batching.Ensemble(chans[0], chans[1], (ns, nc, na, nt), grid, geom,
+                              np.deg2rad(np.linspace(-10, 10, na)), T_START, methods[i])
+        e.build(dev)
+        ens.append(e)
+        shapes.append({"method": methods[i], "depth": depth, "frames": nt, "angles": na})
+    torch.cuda.synchronize()
+    tune_start = time.perf_counter()
+    choice = batching.autotune(ens, sample_tiles=148 * 2, repeats=1)
+    tune_s = time.perf_counter() - tune_start
+    queue = batching.BatchQueue(ens, ctas_per_sm=choice["ctas_per_sm"])
+    queue.capture()
+    for _ in range(max(0, args.warmup - 1)):
+        queue.run()
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = max(1, args.steps)
+    with ClockSampler(0) as sampler:
+        start.record()
+        for _ in range(steps):
+            queue.run()
+        stop.record()
+        torch.cuda.synchronize()
+    clocks = sampler.summary()
+    assert _lib.device_error() == 0
+    queue_ms = start.elapsed_time(stop) / steps
+    done = queue.completion_ms()
+    batch_pd = [e.power().clone() for e in ens]
+    seq_done = batching.sequential(ens)
+    worst = max(float(torch.linalg.vector_norm(b - e.power()) / torch.linalg.vector_norm(e.power()))
+                for b, e in zip(batch_pd, ens))
+    units = sum(e.units() for e in ens)
+    return {
+        "form": "batching", "metric": "ensembles/s, 48-ensemble uneven queue (OPW / XDoppler / DMAS-CCF-ACF)",
+        "value": round(n / (queue_ms / 1e3), 4), "unit": "ensembles/s", "n_gpus": 1, "steps": steps,
+        "warmup": args.warmup, "ms_per_queue": round(queue_ms, 1),
+        "latency_ms": {"p50": round(float(np.percentile(done, 50)), 1),
+                       "p99": round(float(np.percentile(done, 99)), 1)},
+        "gsamples_per_s": round(units / (queue_ms / 1e3) / 1e9, 2),
+        "sequential_plain": {"value": round(n / (seq_done[-1] / 1e3), 4), "unit": "ensembles/s",
+                             "ms_per_queue": round(float(seq_done[-1]), 1),
+                             "latency_ms": {"p50": round(float(np.percentile(seq_done, 50)), 1),
+                                            "p99": round(float(np.percentile(seq_done, 99)), 1)}},
+        "power_rel_l2_batch_vs_sequential_max": worst,
+        "autotune": {**choice, "seconds": round(tune_s, 2)},
+        "latency_definition": "completion time since the queue started (device global timer for the persistent "
+                              "kernel, CUDA events for sequential launches)",
+        "dtype": "f32 math on c64 packed IQ (float64 geometry)", "data": "synthetic seeded complex Gaussian channels",
+        "config": {"workload": "48 ensembles: depth {128,192,256,384} at 128 x depth x 128, frames {50,100,200,400}, "
+                               "128 ch, angles {5,7,11}, ns 512, 50% OPW / 25% XDoppler / 25% DMAS-CCF-ACF",
+                   "seed": args.seed, "ensembles": shapes},
+        "clocks": clocks, "gpu_launches": steps,
+    }
+
+
 # ------------------------------------------------------- CPU (oracle) arms --
 def _oracle_sample(seed: int, voxels: int):
     """A bounded slice of the workload for the float64 CPU oracle: the first voxels of the grid."""
@@ -351,7 +434,15 @@ def main() -> None:
     ap.add_argument("--channels", type=int, default=None, help="reduced channel count for profiling runs")
     ap.add_argument("--subgrid", type=int, nargs=3, default=None, metavar=("NX", "NZ", "NY"),
                     help="central block of the full grid at full resolution (profiling runs)")
+    ap.add_argument("--form", default="filtered", choices=["filtered", "batching"],
+                    help="filtered: the filtered-OPW headline; batching: the uneven-queue form")
+    ap.add_argument("--ensembles", type=int, default=48, help="queue length of the batching form")
+    ap.add_argument("--seed", type=int, default=5, help="seed of the batching queue")
     args = ap.parse_args()
+    if args.form == "batching":
+        if args.impl == "b200" and int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps(run_batching(args)), flush=True)
+        return
     global GRID_SHAPE, NT, NC, SUBGRID
     if args.subgrid:
         SUBGRID = tuple(args.subgrid)

@@ -45,7 +45,30 @@ __device__ __forceinline__ float2 packed_sample(const float2* iq, const Tap& t, 
   return cmul(val, t.phase);
 }
 
+__device__ __forceinline__ Tap shfl_tap(const Tap& t, int src) {
+  Tap o;
+  o.i0 = __shfl_sync(0xffffffffu, t.i0, src);
+  o.w = __shfl_sync(0xffffffffu, t.w, src);
+  o.phase.x = __shfl_sync(0xffffffffu, t.phase.x, src);
+  o.phase.y = __shfl_sync(0xffffffffu, t.phase.y, src);
+  return o;
+}
+
+// Taps of one aperture for channel `outer` (all angles, chan_major = false) or
+// angle `outer` (all channels, chan_major = true), computed one per lane for
+// the 32 inner indices starting at `first`; lanes past the end get an empty tap.
+__device__ __forceinline__ Tap lane_tap(const das::Args& p, const Voxel& q, int config, bool chan_major, int outer,
+                                        int first) {
+  const int inner = first + (threadIdx.x & 31);
+  const int limit = chan_major ? p.nc : p.na;
+  if (inner >= limit) return Tap{-1, 0.f, make_float2(0.f, 0.f)};
+  const int ch = chan_major ? inner : outer, a = chan_major ? outer : inner;
+  return tap_of(q, config, config ? p.ye : p.xe, ch, p.angles, p.starts, a, p.c, p.fs, p.fd, p.fn, p.ns);
+}
+
 // One warp: voxel v (its row in scan / pd / signal), frames [128 fblock, 128 fblock + 128).
+// The float64 taps of every (channel, angle) are formed once per warp, one per
+// lane, and broadcast with shuffles.
 template <int METHOD>
 __device__ void nonlinear_voxel(const das::Args& p, size_t v, int fblock) {
   const int lane = threadIdx.x & 31;
@@ -59,14 +82,18 @@ __device__ void nonlinear_voxel(const das::Args& p, size_t v, int fblock) {
     float2 r[kRegFrames] = {}, s[kRegFrames] = {};
     for (int a = 0; a < p.na; ++a) {
       float2 ar[kRegFrames] = {}, aq[kRegFrames] = {};
-      for (int ch = 0; ch < p.nc; ++ch) {
-        Tap tr = tap_of(q, 0, p.xe, ch, p.angles, p.starts, a, p.c, p.fs, p.fd, p.fn, p.ns);
-        Tap tq = tap_of(q, 1, p.ye, ch, p.angles, p.starts, a, p.c, p.fs, p.fd, p.fn, p.ns);
+      for (int c0 = 0; c0 < p.nc; c0 += 32) {
+        const Tap lr = lane_tap(p, q, 0, true, a, c0), lq = lane_tap(p, q, 1, true, a, c0);
+        const int count = min(32, p.nc - c0);
+        for (int j = 0; j < count; ++j) {
+          const int ch = c0 + j;
+          const Tap tr = shfl_tap(lr, j), tq = shfl_tap(lq, j);
 #pragma unroll
-        for (int f = 0; f < kRegFrames; ++f) {
-          int frame = fbase + 32 * f;
-          ar[f] = cadd(ar[f], packed_sample(rc, tr, ch, a, frame, p.ns, p.na, p.nt));
-          aq[f] = cadd(aq[f], packed_sample(cr, tq, ch, a, frame, p.ns, p.na, p.nt));
+          for (int f = 0; f < kRegFrames; ++f) {
+            int frame = fbase + 32 * f;
+            ar[f] = cadd(ar[f], packed_sample(rc, tr, ch, a, frame, p.ns, p.na, p.nt));
+            aq[f] = cadd(aq[f], packed_sample(cr, tq, ch, a, frame, p.ns, p.na, p.nt));
+          }
         }
       }
 #pragma unroll
@@ -91,14 +118,18 @@ __device__ void nonlinear_voxel(const das::Args& p, size_t v, int fblock) {
     for (int ch = 0; ch < p.nc; ++ch) {
       float2 sr[kRegFrames] = {}, sq[kRegFrames] = {};
       bool act_r = false, act_q = false;
-      for (int a = 0; a < p.na; ++a) {
-        Tap tr = tap_of(q, 0, p.xe, ch, p.angles, p.starts, a, p.c, p.fs, p.fd, p.fn, p.ns);
-        Tap tq = tap_of(q, 1, p.ye, ch, p.angles, p.starts, a, p.c, p.fs, p.fd, p.fn, p.ns);
+      for (int a0 = 0; a0 < p.na; a0 += 32) {
+        const Tap lr = lane_tap(p, q, 0, false, ch, a0), lq = lane_tap(p, q, 1, false, ch, a0);
+        const int count = min(32, p.na - a0);
+        for (int j = 0; j < count; ++j) {
+          const int a = a0 + j;
+          const Tap tr = shfl_tap(lr, j), tq = shfl_tap(lq, j);
 #pragma unroll
-        for (int f = 0; f < kRegFrames; ++f) {
-          int frame = fbase + 32 * f;
-          sr[f] = cadd(sr[f], packed_sample(rc, tr, ch, a, frame, p.ns, p.na, p.nt));
-          sq[f] = cadd(sq[f], packed_sample(cr, tq, ch, a, frame, p.ns, p.na, p.nt));
+          for (int f = 0; f < kRegFrames; ++f) {
+            int frame = fbase + 32 * f;
+            sr[f] = cadd(sr[f], packed_sample(rc, tr, ch, a, frame, p.ns, p.na, p.nt));
+            sq[f] = cadd(sq[f], packed_sample(cr, tq, ch, a, frame, p.ns, p.na, p.nt));
+          }
         }
       }
       receive_delay(q.x, q.z, double(p.xe[ch]), p.c, p.fn, &act_r);
@@ -114,14 +145,18 @@ __device__ void nonlinear_voxel(const das::Args& p, size_t v, int fblock) {
     float er[kRegFrames] = {}, eq[kRegFrames] = {};
     for (int a = 0; a < p.na; ++a) {
       float2 ar[kRegFrames] = {}, aq[kRegFrames] = {};
-      for (int ch = 0; ch < p.nc; ++ch) {
-        Tap tr = tap_of(q, 0, p.xe, ch, p.angles, p.starts, a, p.c, p.fs, p.fd, p.fn, p.ns);
-        Tap tq = tap_of(q, 1, p.ye, ch, p.angles, p.starts, a, p.c, p.fs, p.fd, p.fn, p.ns);
+      for (int c0 = 0; c0 < p.nc; c0 += 32) {
+        const Tap lr = lane_tap(p, q, 0, true, a, c0), lq = lane_tap(p, q, 1, true, a, c0);
+        const int count = min(32, p.nc - c0);
+        for (int j = 0; j < count; ++j) {
+          const int ch = c0 + j;
+          const Tap tr = shfl_tap(lr, j), tq = shfl_tap(lq, j);
 #pragma unroll
-        for (int f = 0; f < kRegFrames; ++f) {
-          int frame = fbase + 32 * f;
-          ar[f] = cadd(ar[f], packed_sample(rc, tr, ch, a, frame, p.ns, p.na, p.nt));
-          aq[f] = cadd(aq[f], packed_sample(cr, tq, ch, a, frame, p.ns, p.na, p.nt));
+          for (int f = 0; f < kRegFrames; ++f) {
+            int frame = fbase + 32 * f;
+            ar[f] = cadd(ar[f], packed_sample(rc, tr, ch, a, frame, p.ns, p.na, p.nt));
+            aq[f] = cadd(aq[f], packed_sample(cr, tq, ch, a, frame, p.ns, p.na, p.nt));
+          }
         }
       }
 #pragma unroll
