@@ -333,7 +333,11 @@ def run_batching(args) -> dict:
     worst = max(float(torch.linalg.vector_norm(b - e.power()) / torch.linalg.vector_norm(e.power()))
                 for b, e in zip(batch_pd, ens))
     units = sum(e.units() for e in ens)
+    durations = np.diff(np.concatenate(([0.0], seq_done)))
+    by_method = {m: round(float(sum(d for d, e in zip(durations, ens) if e.method == m)), 1)
+                 for m in ("opw", "xdoppler", "dmas")}
     return {
+        "sequential_ms_by_method": by_method,
         "form": "batching", "metric": "ensembles/s, 48-ensemble uneven queue (OPW / XDoppler / DMAS-CCF-ACF)",
         "value": round(n / (queue_ms / 1e3), 4), "unit": "ensembles/s", "n_gpus": 1, "steps": steps,
         "warmup": args.warmup, "ms_per_queue": round(queue_ms, 1),

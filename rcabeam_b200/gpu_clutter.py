@@ -25,7 +25,7 @@ from time import perf_counter
 import numpy as np
 import torch
 
-from rcabeam_b200 import _lib
+from rcabeam_b200 import _lib, sharded
 
 _GRAM_PRECISION = {"complex128": 0, "complex64": 1, "tf32": 2, "bf16x3": 3}
 # Machine epsilon of the Gram's products, for the negative-eigenvalue tolerance
@@ -86,8 +86,12 @@ class Gram:
         _lib.check(_lib.lib().rcabeam_heevd_workspace_bytes(frames, ctypes.byref(size)), "heevd_workspace")
         self.workspace = torch.empty(max(int(size.value), 16), dtype=torch.uint8, device=device)
 
-    def accumulate(self, arrays, precision: str) -> int:
-        """Scale, then Gram of every array into one shared matrix; returns total rows."""
+    def accumulate(self, arrays, precision: str, group=None) -> int:
+        """Scale, then Gram of every array into one shared matrix; returns total rows.
+
+        With a process group the rows are spread over its ranks: the scale is
+        the maximum and the Gram the sum over all ranks (rcabeam_b200.sharded).
+        """
         prec = _GRAM_PRECISION[precision]
         if prec >= 2 and (any(a.dtype != torch.complex64 for a in arrays) or self.frames % 2 or self.frames > 1024):
             raise ValueError(f"Precision {precision} requires complex64 IQ with an even frame count <= 1024")
@@ -95,12 +99,14 @@ class Gram:
         self.upper.zero_()
         for a in arrays:
             _lib.call("rcabeam_clutter_scale_device", a.data_ptr(), a.numel(), _is128(a), self.scale.data_ptr())
+        sharded.reduce_scale(self.scale, group)
         rows = 0
         for a in arrays:
             m = _rows(a)
             _lib.call("rcabeam_gram_accumulate_device", m.data_ptr(), m.shape[0], self.frames, _is128(m),
                       self.scale.data_ptr(), prec, self.upper.data_ptr())
             rows += m.shape[0]
+        rows = sharded.reduce_gram(self.upper, rows, group)
         _lib.call("rcabeam_gram_finish_device", self.upper.data_ptr(), self.matrix.data_ptr(), self.frames, rows)
         return rows
 
@@ -117,10 +123,11 @@ class Gram:
 
 
 def temporal_basis(iq, *, method: str = "gram", precision: str = "complex128", timings: dict | None = None,
-                   diagnostics: dict | None = None) -> tuple[torch.Tensor, torch.Tensor]:
+                   diagnostics: dict | None = None, group=None) -> tuple[torch.Tensor, torch.Tensor]:
     """Descending singular values (T,) and column temporal vectors V (T, T) (gpu_clutter.py:112-193).
 
-    A tuple of arrays estimates one shared basis over all of their rows.
+    A tuple of arrays estimates one shared basis over all of their rows; with a
+    torch.distributed process group, over the rows of every rank of the group.
     """
     arrays = _inputs(iq)
     frames = arrays[0].shape[-1]
@@ -130,7 +137,7 @@ def temporal_basis(iq, *, method: str = "gram", precision: str = "complex128", t
         raise ValueError("Method must be 'gram'")
     begin = perf_counter()
     gram = Gram(frames, arrays[0].device)
-    rows = gram.accumulate(arrays, precision)
+    rows = gram.accumulate(arrays, precision, group)
     matrix = torch.view_as_real(gram.vectors())
     if not bool(torch.isfinite(matrix).all()):
         raise np.linalg.LinAlgError("Nonfinite Gram matrix; rescale the IQ input")

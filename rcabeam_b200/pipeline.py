@@ -7,7 +7,10 @@ clutter-filtered power Doppler.  All buffers are allocated once; ``run``
 launches every stage on the default stream without host synchronization
 except the final solver-status check, and records CUDA events per stage.
 ``run_host`` adds the pinned host -> device upload of the channels and the
-device -> host read of the power, the boundary a host caller sees.
+device -> host read of the power, the boundary a host caller sees.  With a
+process group, each rank reconstructs its x slab of the grid
+(``sharded.shard_grid``) and the clutter basis is estimated over every rank's
+rows (one MAX and one SUM all-reduce, ``rcabeam_b200.sharded``).
 """
 
 from __future__ import annotations
@@ -26,7 +29,8 @@ class FilteredOpw:
     """Fixed-shape filtered-OPW pipeline: ``run(rc, cr) -> (nx, nz, ny)`` float64 filtered power."""
 
     def __init__(self, channel_shape, angles, t_start, grid, geom: RCAGeometry, *, rank_start: int = 3,
-                 rank_stop: int | None = None, precision: str = "complex128", iq_storage: str = "float32"):
+                 rank_stop: int | None = None, precision: str = "complex128", iq_storage: str = "float32",
+                 group=None):
         ns, nc, na, nt = (int(n) for n in channel_shape)
         self.shape = (len(grid[0]), len(grid[1]), len(grid[2]))
         self.channel_shape = (ns, nc, na, nt)
@@ -35,6 +39,7 @@ class FilteredOpw:
             raise ValueError("Require 0 <= rank_start <= rank_stop <= number of frames")
         self.rank = (int(rank_start), stop)
         self.precision = precision
+        self.group = group  # process group whose ranks hold the other x slabs (rcabeam_b200.sharded)
         if iq_storage not in ("float32", "float16", "bf16x2"):
             raise ValueError("IQ storage must be float32, float16 or bf16x2")
         if iq_storage == "bf16x2" and nt % 4:
@@ -110,7 +115,7 @@ class FilteredOpw:
                                        self.starts, self.pd, self.iq, self.geometry, ns, nc, na, nt, *self.consts,
                                        self.half, synchronize=False)
         ev[2].record()
-        self.gram.accumulate((self.iq,), self.precision)
+        self.gram.accumulate((self.iq,), self.precision, self.group)
         ev[3].record()
         self.gram.decompose()
         ev[4].record()
