@@ -122,7 +122,7 @@ def peaks() -> dict:
 # ----------------------------------------------------------------- B200 arm --
 FORMS = {
     # name: (packed IQ storage, Gram precision)
-    "chosen": ("bf16x2", "complex128"),
+    "chosen": ("bf16x2", "bf16x3"),
     "plain": ("float32", "complex128"),
     "fp16_storage": ("float16", "complex128"),
 }
@@ -248,7 +248,8 @@ def run_b200(args, rank: int, world: int) -> dict | None:
         "metric": "OPW Gsamples/s (vox*ch*ang*frm), filtered PD", "value": ch["gsamples_per_s"],
         "unit": "Gsamples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ch["ms_per_ensemble"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 math on bf16x2-split c64 IQ (tcgen05 3-product DAS), f64 Gram/eig/projection",
+        "dtype": "f32 math on bf16x2-split c64 IQ (tcgen05 3-product DAS), 3xBF16 tcgen05 Gram with f64 flushes, "
+                 "f64 eig/projection",
         "data": "synthetic seeded channel IQ (complex Gaussian), full-size shapes", "config": CONFIG,
         "filtered_pd_ms_per_ensemble": {"chosen": ch["ms_per_ensemble"],
                                          **({"plain": results["plain"]["ms_per_ensemble"]} if "plain" in results else {})},
@@ -360,6 +361,128 @@ def run_batching(args) -> dict:
     }
 
 
+# ------------------------------------------------------ precision form --
+def run_precision(args) -> dict:
+    """Casorati 4,194,304 x 400 complex64 clutter scene: Gram in float64 / float32 CUDA cores and
+    TF32 / 3xBF16 tensor cores, float64 EVD and projection; errors against the float64 Gram."""
+    import torch
+
+    from rcabeam_b200 import _lib, gpu_clutter, scenes
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    rows, frames = args.rows, args.casorati_frames
+    gen = torch.Generator(device=dev).manual_seed(args.seed)
+    iq = scenes.clutter_casorati(rows, frames, generator=gen, device=dev)
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    gram = gpu_clutter.Gram(frames, dev)
+    out, ref_pd, ref_iq = {}, None, None
+    for precision in ("complex128", "complex64", "tf32", "bf16x3"):
+        for _ in range(max(1, args.warmup)):
+            gram.accumulate((iq,), precision)
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(max(1, args.steps)):
+            gram.accumulate((iq,), precision)
+        stop.record()
+        torch.cuda.synchronize()
+        gram_ms = start.elapsed_time(stop) / max(1, args.steps)
+        start.record()
+        _, basis = gpu_clutter.temporal_basis(iq, precision=precision)
+        stop.record()
+        torch.cuda.synchronize()
+        basis_ms = start.elapsed_time(stop)
+        start.record()
+        pd = gpu_clutter.filtered_power(iq, basis, rank_start=3)
+        stop.record()
+        torch.cuda.synchronize()
+        power_ms = start.elapsed_time(stop)
+        filtered = gpu_clutter.apply_temporal_filter(iq, basis, rank_start=3)
+        entry = {"gram_ms": round(gram_ms, 2), "basis_ms_incl_gram_evd": round(basis_ms, 2),
+                 "filtered_power_ms": round(power_ms, 2),
+                 "gram_tflops_upper": round(4 * rows * frames * (frames + 64) / gram_ms / 1e9, 1)}
+        if precision == "complex128":
+            ref_pd, ref_iq = pd, filtered
+        else:
+            entry["filtered_pd_rel_l2_vs_f64"] = float(torch.linalg.vector_norm(pd - ref_pd)
+                                                       / torch.linalg.vector_norm(ref_pd))
+            entry["filtered_iq_rel_l2_vs_f64"] = float(torch.linalg.vector_norm((filtered - ref_iq).abs())
+                                                       / torch.linalg.vector_norm(ref_iq.abs()))
+        out[precision] = entry
+        del filtered
+        torch.cuda.empty_cache()
+    assert _lib.device_error() == 0
+    return {"form": "precision", "metric": "Gram ms (Casorati rows x frames, complex64)", "forms": out,
+            "reference": "float64 CUDA-core Gram + float64 EVD + float64 projection on the GPU (pinned to the "
+                         "NumPy complex128 oracle in tests)",
+            "config": {"workload": f"clutter scene Casorati {rows} x {frames} c64 (rank-3 tissue 0/-6/-12 dB, "
+                                   "blood -40 dB in 2 % of rows, noise -50 dB), rank_start=3", "seed": args.seed},
+            "data": "synthetic seeded scene model", "gpu_launches": None}
+
+
+# ------------------------------------------------ differentiation form --
+def run_differentiation(args) -> dict:
+    """Grid 64 x 128 x 64, channels (384, 128, 7, 32): forward PD of the whole grid and the
+    backward of the 1 mm ROI loss through the hand-written adjoint, complex64 channels."""
+    import torch
+
+    from rcabeam_b200 import _lib
+    from rcabeam_b200.autograd import DasGeometry, OpwPowerDoppler
+    from rcabeam_b200.sim import RCAGeometry, scan_coords, simulate_point
+
+    torch.cuda.set_device(0)
+    ns, nc, na, nt = 384, 128, 7, 32
+    el = (np.arange(nc) - (nc - 1) / 2) * PITCH
+    half = (nc - 1) / 2 * PITCH
+    geom = RCAGeometry(el, el, c=C, fs=FS, f_demod=FD, fnumber=None)
+    angles = np.deg2rad(np.linspace(-10, 10, na))
+    target = (0.35e-3, 8.0e-3, -0.22e-3)
+    rng = np.random.default_rng(args.seed)
+    phases = np.exp(2j * np.pi * rng.random(nt))
+    chans = []
+    for config in ("RC", "CR"):
+        data = simulate_point(geom, angles, target, ns, T_START, config)
+        noise = 0.01 * (rng.normal(size=(ns, nc, na, nt)) + 1j * rng.normal(size=(ns, nc, na, nt)))
+        chans.append(torch.from_numpy((data[..., None] * phases + noise).astype(np.complex64)).cuda())
+    grid = (np.linspace(-half, half, 64), np.linspace(4e-3, 12e-3, 128), np.linspace(-half, half, 64))
+    geometry = DasGeometry.build(grid, geom, angles, T_START)
+    scan = scan_coords(grid)
+    roi = torch.from_numpy((np.sum((scan - np.array(target)) ** 2, axis=1) <= 1e-6).astype(np.float64)).cuda()
+    offsets = torch.from_numpy(rng.normal(scale=5e-9, size=(2, nc))).cuda()
+    rc = chans[0].requires_grad_()
+    off = offsets.clone().requires_grad_()
+    c = torch.tensor(1523.0, dtype=torch.float64, device="cuda", requires_grad=True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    fwd, bwd = [], []
+    for step in range(max(1, args.warmup) + max(1, args.steps)):
+        rc.grad = off.grad = c.grad = None
+        ev[0].record()
+        pd = OpwPowerDoppler.apply(rc, chans[1], off, c, geometry, 8)
+        loss = (pd * roi).sum()
+        ev[1].record()
+        loss.backward()
+        ev[2].record()
+        torch.cuda.synchronize()
+        if step >= max(1, args.warmup):
+            fwd.append(ev[0].elapsed_time(ev[1]))
+            bwd.append(ev[1].elapsed_time(ev[2]))
+    assert _lib.device_error() == 0
+    units = geometry.voxels * 2 * nc * na * nt
+    roi_units = int(roi.sum().item()) * 2 * nc * na * nt
+    f_ms, b_ms = statistics.median(fwd), statistics.median(bwd)
+    return {"form": "differentiation", "metric": "forward Gsamples/s (whole grid) and backward ms (ROI loss)",
+            "forward_ms": round(f_ms, 2), "forward_gsamples_per_s": round(units / f_ms / 1e6, 1),
+            "backward_ms": round(b_ms, 2), "roi_voxels": int(roi.sum().item()),
+            "backward_gsamples_per_s": round(2 * roi_units / b_ms / 1e6, 2),
+            "note": "backward recomputes the ROI IQ (forward units) and scatters the adjoint (same units again)",
+            "dtype": "complex64 channels, float32 interpolation, float64 geometry and gradient sums",
+            "config": {"workload": "grid 64x128x64 over +-7 mm x 4-12 mm, channels (384,128,7,32), point target, "
+                                   "loss = sum PD over a 1 mm sphere, offsets N(0, 5 ns), c = 1523 m/s",
+                       "seed": args.seed},
+            "data": "simulated point target + noise"}
+
+
 # ------------------------------------------------------- CPU (oracle) arms --
 def _oracle_sample(seed: int, voxels: int):
     """A bounded slice of the workload for the float64 CPU oracle: the first voxels of the grid."""
@@ -438,14 +561,17 @@ def main() -> None:
     ap.add_argument("--channels", type=int, default=None, help="reduced channel count for profiling runs")
     ap.add_argument("--subgrid", type=int, nargs=3, default=None, metavar=("NX", "NZ", "NY"),
                     help="central block of the full grid at full resolution (profiling runs)")
-    ap.add_argument("--form", default="filtered", choices=["filtered", "batching"],
-                    help="filtered: the filtered-OPW headline; batching: the uneven-queue form")
+    ap.add_argument("--form", default="filtered", choices=["filtered", "batching", "precision", "differentiation"],
+                    help="filtered: the filtered-OPW headline; batching, precision, differentiation: the forms")
+    ap.add_argument("--rows", type=int, default=128 * 256 * 128, help="Casorati rows of the precision form")
+    ap.add_argument("--casorati-frames", type=int, default=400, help="Casorati frames of the precision form")
     ap.add_argument("--ensembles", type=int, default=48, help="queue length of the batching form")
     ap.add_argument("--seed", type=int, default=5, help="seed of the batching queue")
     args = ap.parse_args()
-    if args.form == "batching":
+    if args.form != "filtered":
         if args.impl == "b200" and int(os.environ.get("RANK", "0")) == 0:
-            print(json.dumps(run_batching(args)), flush=True)
+            run = {"batching": run_batching, "precision": run_precision, "differentiation": run_differentiation}
+            print(json.dumps(run[args.form](args)), flush=True)
         return
     global GRID_SHAPE, NT, NC, SUBGRID
     if args.subgrid:

@@ -181,7 +181,7 @@ rcabeam_status rcabeam_clutter_scale_device(const void* iq, size_t n, int comple
  * into upper (device, row-major nt x nt complex128, zeroed by the caller).
  * precision: 0 float64 CUDA cores, 1 float32 CUDA cores, 2 TF32 tensor cores,
  * 3 3xBF16 tensor cores.  Precisions 2 and 3 (tcgen05, float32 accumulation
- * flushed to float64 every 16384 rows) need complex64 rows (complex128 = 0),
+ * flushed to float64 every 2048 rows) need complex64 rows (complex128 = 0),
  * an even nt <= 1024, rows < 2^31 and a 16-byte aligned iq; they scale X by
  * the power of two that bounds s before rounding, so the sum stays in range.
  * Call once per array to estimate one shared basis (gpu_clutter.py:144-160). */

@@ -53,7 +53,10 @@ constexpr int kRing = 2;           // staging and operand ring depth
 constexpr int kThreads = 256;
 constexpr int kConverters = 6 * 32;
 constexpr int kSlotBytes = kBlock * kRows * 4;  // 8192: one staged block per stage (f32 or bf16 hi+lo)
-constexpr int kFlushRows = 16384;
+// The tensor core rounds each float32 accumulation toward zero (a shrink of
+// ~1.3e-8 per update); flushing to float64 every 2048 rows (256 TF32 or 384
+// BF16 updates) keeps that bias near 3e-6 of a Gram entry.
+constexpr int kFlushRows = 2048;
 constexpr int kTmemCols = 512;
 // MN-major TF32 operands take the 128-byte swizzle with 32-byte granules (the
 // TMA's SWIZZLE_128B_ATOM_32B): 4-row K atoms, so SBO = 512 B; BF16 operands

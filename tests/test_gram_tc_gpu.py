@@ -5,7 +5,7 @@ product of its (rows, 2T) float32 view.  Bars (relative Frobenius error of the
 finished Gram against float64, tolerances in the tests):
   * TF32 (10-bit mantissa operands, round to nearest): <= 1e-3;
   * 3xBF16 (hi/lo split, three products): <= 3e-5;
-both with float32 accumulation flushed to float64 every 16384 rows.
+both with float32 accumulation flushed to float64 every 2048 rows.
 Shapes cover frame counts that are not multiples of 64 (ragged last block),
 row counts that are not multiples of 16 (ragged last stage), more than one
 flush per CTA, and data scaled far from 1 (the power-of-two prescale).
