@@ -53,7 +53,8 @@ namespace tc {
 constexpr int kVox = 128;          // voxels per tile
 constexpr int kGroupVox = 64;      // voxels per M=128 MMA block
 constexpr int kRows = 16;
-constexpr int kStages = 4;
+constexpr int kStages = 4;         // ring depth when five stages do not fit shared memory
+constexpr int kDeepStages = 5;     // ring depth otherwise (decouples builders from the MMA)
 constexpr int kBoxCols = 64;       // 16-bit columns per TMA box (one 128-byte swizzle atom)
 constexpr int kBoxBytes = kBoxCols * 2 * kRows;  // 2048
 constexpr int kMaxFrames = 128;    // frames per pass: 2 x frames columns <= 256 per group
@@ -61,6 +62,10 @@ constexpr int kBuilders = 4;       // builder warps
 constexpr int kMmaWarp = kBuilders;
 constexpr int kThreads = (kBuilders + 1 + 4) * 32;
 constexpr int kTmemCols = 512;     // group g accumulates in columns [256 g, 256 g + 2F)
+// Builders claim ring positions from a shared counter and wait for a stage by
+// mbarrier parity, which is unambiguous only while a waiter is at most one
+// phase ahead: that holds when no more builders than stages hold claims.
+static_assert(kBuilders <= kStages && kStages <= kDeepStages, "every builder needs its own ring stage");
 constexpr int kAMatBytes = 128 * kRows * 2;  // 4096: one 128 x 16 16-bit matrix
 // FP16 coefficients (|c| <= 1) are scaled by 2^10 before the hi/lo split so that
 // the lo halves of small coefficients stay out of the FP16 subnormal range; the
@@ -111,8 +116,8 @@ struct Layout {
   }
   // stages | control (barriers, meta, counter, TMEM slot) | angle table |
   // per-tile transmit delays [2][na][128] double | transmit phases [2][na][128] float2
-  static size_t bytes(int nbox, int na) {
-    return kStages * stage_bytes(nbox) + 1024 + size_t(na) * 3 * sizeof(double) + size_t(na) * 2 * kVox * 16 +
+  static size_t bytes(int nbox, int na, int stages) {
+    return size_t(stages) * stage_bytes(nbox) + 1024 + size_t(na) * 3 * sizeof(double) + size_t(na) * 2 * kVox * 16 +
            1024;
   }
 };
@@ -220,10 +225,11 @@ __device__ __forceinline__ float2 demod_phase(double fd, double tau) {
   return make_float2(cs, sn);
 }
 
-template <bool BF16X3>
+template <bool BF16X3, int STAGES>
 __global__ void __launch_bounds__(kThreads, 1)
     opw_tc(const __grid_constant__ CUtensorMap map_rc_hi, const __grid_constant__ CUtensorMap map_cr_hi,
            const __grid_constant__ CUtensorMap map_rc_lo, const __grid_constant__ CUtensorMap map_cr_lo, Args p) {
+  static_assert(kBuilders <= STAGES, "every builder needs its own ring stage");
   using L = Layout<BF16X3>;
   constexpr int kPlanes = L::kPlanes;
   constexpr int kProducts = BF16X3 ? 3 : 2;
@@ -232,14 +238,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const size_t stage_bytes = L::stage_bytes(p.nbox);
   unsigned char* stages = smem;
-  unsigned char* ctrl = smem + kStages * stage_bytes;
+  unsigned char* ctrl = smem + STAGES * stage_bytes;
   uint64_t* full = reinterpret_cast<uint64_t*>(ctrl);
-  uint64_t* empty = full + kStages;
-  uint64_t* acc_full = empty + kStages;
+  uint64_t* empty = full + STAGES;
+  uint64_t* acc_full = empty + STAGES;
   uint64_t* acc_empty = acc_full + 1;
   uint64_t* drain = acc_empty + 1;
   int* meta = reinterpret_cast<int*>(drain + 1);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(meta + kStages);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(meta + STAGES);
   int* counter = reinterpret_cast<int*>(tmem_slot + 1);  // next ring stage to claim
   int* item_steps = counter + 1;                         // steps staged for the current item
   volatile int* acc_kind = item_steps + 1;               // AccKind of the pending flush
@@ -249,7 +255,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], 32);  // the writing builder warp
       mbar_init(&empty[s], 1);  // tcgen05.commit (or a plain arrive for markers)
     }
@@ -297,7 +303,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (lane == 0) mine = uint32_t(atomicAdd(counter, 1));
       k = __shfl_sync(0xffffffffu, mine, 0);
       return __all_sync(0xffffffffu,
-                        mbar_wait(&empty[k % kStages], ((k / kStages) & 1) ^ 1, p.err, kErrWaitEmpty));
+                        mbar_wait(&empty[k % STAGES], ((k / STAGES) & 1) ^ 1, p.err, kErrWaitEmpty));
     };
     // Stages the window [row, row + 16) x [col0, col0 + ncols) of every plane.
     auto stage_window = [&](uint32_t s, unsigned char* stage, int config, int col0, int row, int slab) {
@@ -393,7 +399,7 @@ __global__ void __launch_bounds__(kThreads, 1)
               uint32_t k = 0;
               if (ok) ok = claim(k);
               if (!ok) continue;  // failed: keep the control flow, skip the work
-              const uint32_t s = k % kStages;
+              const uint32_t s = k % STAGES;
               unsigned char* stage = stages + size_t(s) * stage_bytes;
 #pragma unroll
               for (int j = 0; j < 4; ++j) {
@@ -428,7 +434,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           uint32_t k = 0;
           if (ok) ok = claim(k);
           if (ok) {
-            const uint32_t s = k % kStages;
+            const uint32_t s = k % STAGES;
             unsigned char* stage = stages + size_t(s) * stage_bytes;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
@@ -444,8 +450,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         uint32_t k = 0;
         if (ok) ok = claim(k);
         if (ok) {
-          if (lane == 0) meta[k % kStages] = kTileEnd;
-          mbar_arrive(&full[k % kStages]);
+          if (lane == 0) meta[k % STAGES] = kTileEnd;
+          mbar_arrive(&full[k % STAGES]);
         }
       }
     }
@@ -454,14 +460,14 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t k = 0;
       if (ok) ok = claim(k);
       if (ok) {
-        if (lane == 0) meta[k % kStages] = kFinish;
-        mbar_arrive(&full[k % kStages]);
+        if (lane == 0) meta[k % STAGES] = kFinish;
+        mbar_arrive(&full[k % STAGES]);
       }
       // Drain: the copies of the last stages (globally last, so no later phase
       // exists on their barriers) have landed before the builders leave.
       const uint32_t total = uint32_t(*counter);
-      for (uint32_t u = total > kStages ? total - kStages : 0; u < total; ++u)
-        mbar_wait(&full[u % kStages], (u / kStages) & 1, p.err, kErrWaitDrain);
+      for (uint32_t u = total > STAGES ? total - STAGES : 0; u < total; ++u)
+        mbar_wait(&full[u % STAGES], (u / STAGES) & 1, p.err, kErrWaitDrain);
     }
   } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------------- MMA --
@@ -481,8 +487,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         seg = 0;
       };
       for (;;) {
-        const int s = k % kStages;
-        if (!mbar_wait(&full[s], (k / kStages) & 1, p.err, kErrWaitFull)) break;
+        const int s = k % STAGES;
+        if (!mbar_wait(&full[s], (k / STAGES) & 1, p.err, kErrWaitFull)) break;
         const int m = meta[s];
         if (m == kFinish) break;
         if (need_empty) {

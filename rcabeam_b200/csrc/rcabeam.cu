@@ -251,11 +251,13 @@ static bool tc_eligible(const void* const* planes, int count, size_t nt) {
 }
 
 // Shared memory of the tensor-core OPW for nt frames and na angles (0 if it cannot run).
-static size_t tc_smem_bytes(bool bf16x3, size_t nt, size_t na) {
+// Shared memory of the tensor-core kernel with `stages` ring stages (0: does not fit).
+static size_t tc_smem_bytes(bool bf16x3, size_t nt, size_t na, int stages = tc::kStages) {
   const size_t chunks = (nt + tc::kMaxFrames - 1) / tc::kMaxFrames;
   const size_t frames = ((nt + chunks - 1) / chunks + 7) / 8 * 8;
   const int nbox = int((2 * frames + tc::kBoxCols - 1) / tc::kBoxCols);
-  size_t smem = (bf16x3 ? tc::Layout<true>::bytes(nbox, int(na)) : tc::Layout<false>::bytes(nbox, int(na))) + 1024;
+  size_t smem = (bf16x3 ? tc::Layout<true>::bytes(nbox, int(na), stages)
+                        : tc::Layout<false>::bytes(nbox, int(na), stages)) + 1024;
   if (smem < 120 * 1024) smem = 120 * 1024;  // one CTA per SM: each owns all 512 TMEM columns
   return smem <= 227 * 1024 ? smem : 0;
 }
@@ -282,7 +284,8 @@ static float2* tc_partials_address() {
 template <bool BF16X3>
 static rcabeam_status run_tc(tc::Args a) {
   const size_t nt = size_t(a.nt);
-  const size_t smem = tc_smem_bytes(BF16X3, nt, size_t(a.na));
+  const size_t deep = tc_smem_bytes(BF16X3, nt, size_t(a.na), tc::kDeepStages);
+  const size_t smem = deep ? deep : tc_smem_bytes(BF16X3, nt, size_t(a.na));
   if (!smem) return RCABEAM_ERROR_ARGUMENT;
   a.chunks = int((nt + tc::kMaxFrames - 1) / tc::kMaxFrames);
   int frames = int((nt + a.chunks - 1) / a.chunks);
@@ -304,7 +307,7 @@ static rcabeam_status run_tc(tc::Args a) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  auto kern = tc::opw_tc<BF16X3>;
+  auto kern = deep ? tc::opw_tc<BF16X3, tc::kDeepStages> : tc::opw_tc<BF16X3, tc::kStages>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
     return RCABEAM_ERROR_CUDA;
   a.partial = tc_partials_address();
