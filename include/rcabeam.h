@@ -242,7 +242,17 @@ rcabeam_status rcabeam_opw_offsets_forward_device(const void* rc, const void* cr
                                                   size_t ns, size_t nc, size_t na, size_t nt, size_t frame0,
                                                   size_t frames, void* iq, double* power, int complex128);
 
-/* Adjoint of the forward above for the upstream gradient grad_iq (nvl x frames,
+/* Power of the same model over nv voxels and every frame, from PACKED complex64
+ * channels (rcabeam_pack_ensemble_device) on the TMA-staged float32 DAS: pd
+ * (2 * nv floats, result in the even entries).  workspace: at least
+ * rcabeam_ensemble_workspace_bytes(nv, nc, na) bytes (traversal order). */
+rcabeam_status rcabeam_opw_offsets_power_device(const void* rc, const void* cr, const float* scan, const float* xe,
+                                                const float* ye, const float* angles, const float* starts,
+                                                const double* offsets, double c, float fs, float fd, float fn,
+                                                size_t ns, size_t nc, size_t na, size_t nt, size_t nv, float* pd,
+                                                void* workspace, size_t workspace_bytes);
+
+/* Adjoint of rcabeam_opw_offsets_forward_device for the upstream gradient grad_iq (nvl x frames,
  * dL/dRe + j dL/dIm): adds to grad_rc / grad_cr (user layout, channels' type;
  * atomics), grad_offsets (2 * nc float64) and *grad_c (float64). */
 rcabeam_status rcabeam_opw_offsets_adjoint_device(const void* rc, const void* cr, const float* scan,

@@ -45,6 +45,7 @@ SIGNATURES: dict[str, list] = {
     "rcabeam_ensemble_static_device": [P, P, P, P, P, P, P, P, P, Z, Z, Z, Z, Z, F, F, F, F, I],
     "rcabeam_ensemble_workspace_bytes": [Z, Z, Z, ctypes.POINTER(c_size_t)],
     "rcabeam_opw_offsets_forward_device": [P, P, P, P, Z, P, P, P, P, P, D, F, F, F, Z, Z, Z, Z, Z, Z, P, P, I],
+    "rcabeam_opw_offsets_power_device": [P, P, P, P, P, P, P, P, D, F, F, F, Z, Z, Z, Z, Z, P, P, Z],
     "rcabeam_opw_offsets_adjoint_device": [P, P, P, P, Z, P, P, P, P, P, D, F, F, F, Z, Z, Z, Z, Z, Z, P, P, P, P, P,
                                            I],
     "rcabeam_batch_table_bytes": [Z, P, ctypes.POINTER(c_size_t)],

@@ -8,8 +8,10 @@ with two extra parameters: a delay offset per receive element of each aperture
 channel IQ of both apertures, the offsets and the sound speed through the
 hand-written adjoint kernels of the C ABI (``rcabeam_opw_offsets_*``).
 
-Memory: neither pass keeps the beamformed ensemble.  The forward accumulates
-power chunk by chunk over ``frame_chunk`` frames (at most 8); the backward
+Memory: neither pass keeps the beamformed ensemble.  For complex64 channels
+the forward packs both apertures and runs the TMA-staged DAS with the offsets
+(power only); for complex128 it accumulates power chunk by chunk over
+``frame_chunk`` frames (at most 8) with the float64 kernel.  The backward
 recomputes, chunk by chunk, the IQ of the voxels whose upstream gradient is
 nonzero, forms dL/dIQ = 2 g IQ / nt and scatters it with the adjoint.  The
 backward cost therefore scales with the number of voxels that carry gradient
@@ -22,6 +24,7 @@ channels run float64 throughout (the finite-difference checker).
 
 from __future__ import annotations
 
+import ctypes
 from dataclasses import dataclass
 
 import numpy as np
@@ -86,6 +89,26 @@ def _geometry_args(geometry, voxels, nvl, offsets, c, shape, frame0, frames):
             geometry.fs, geometry.fd, geometry.fn, ns, nc, na, nt, frame0, frames)
 
 
+def _staged_power(rc, cr, offsets, c, geometry) -> torch.Tensor:
+    """Whole-grid power of complex64 channels on the TMA-staged DAS (packs both apertures first)."""
+    ns, nc, na, nt = rc.shape
+    nv = geometry.voxels
+    packed = []
+    for src in (rc, cr):
+        dst = torch.empty_like(src)
+        _lib.call("rcabeam_pack_ensemble_device", src.data_ptr(), dst.data_ptr(), ns, nc, na, nt)
+        packed.append(dst)
+    size = ctypes.c_size_t(0)
+    _lib.check(_lib.lib().rcabeam_ensemble_workspace_bytes(nv, nc, na, ctypes.byref(size)), "workspace_bytes")
+    work = torch.empty(int(size.value), dtype=torch.uint8, device=rc.device)
+    pd = torch.empty((nv, 2), dtype=torch.float32, device=rc.device)
+    _lib.call("rcabeam_opw_offsets_power_device", packed[0].data_ptr(), packed[1].data_ptr(), geometry.scan.data_ptr(),
+              geometry.xe.data_ptr(), geometry.ye.data_ptr(), geometry.angles.data_ptr(), geometry.starts.data_ptr(),
+              offsets.data_ptr(), c, geometry.fs, geometry.fd, geometry.fn, ns, nc, na, nt, nv, pd.data_ptr(),
+              work.data_ptr(), work.numel())
+    return pd[:, 0].to(torch.float64)
+
+
 class OpwPowerDoppler(torch.autograd.Function):
     """PD (nv,) float64 of the offset-extended OPW model; see the module docstring."""
 
@@ -99,12 +122,15 @@ class OpwPowerDoppler(torch.autograd.Function):
         c = float(sound_speed.item())
         nt = rc.shape[3]
         is128 = int(rc.dtype == torch.complex128)
-        pd = torch.zeros(geometry.voxels, dtype=torch.float64, device=rc.device)
-        for f0 in range(0, nt, frame_chunk):
-            frames = min(frame_chunk, nt - f0)
-            _lib.call("rcabeam_opw_offsets_forward_device", rc.data_ptr(), cr.data_ptr(),
-                      *_geometry_args(geometry, None, geometry.voxels, offsets, c, rc.shape, f0, frames), None,
-                      pd.data_ptr(), is128)
+        if is128:
+            pd = torch.zeros(geometry.voxels, dtype=torch.float64, device=rc.device)
+            for f0 in range(0, nt, frame_chunk):
+                frames = min(frame_chunk, nt - f0)
+                _lib.call("rcabeam_opw_offsets_forward_device", rc.data_ptr(), cr.data_ptr(),
+                          *_geometry_args(geometry, None, geometry.voxels, offsets, c, rc.shape, f0, frames), None,
+                          pd.data_ptr(), is128)
+        else:
+            pd = _staged_power(rc, cr, offsets, c, geometry)
         ctx.save_for_backward(rc, cr, offsets)
         ctx.geometry, ctx.c, ctx.chunk = geometry, c, frame_chunk
         return pd

@@ -53,6 +53,7 @@ struct Args {
   double c, fs, fd, fn;
   int frame_base;  // first frame of chunk 0 of this launch
   int* err;
+  const double* offsets;  // [2][nc] receive-delay offsets in seconds (RC, CR), or nullptr
 };
 
 struct alignas(16) StageTap {
@@ -144,6 +145,7 @@ __device__ bool produce_item(const CUtensorMap* map_rc, const CUtensorMap* map_c
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
         trx[j] = receive_delay(config ? py[j] : px[j], pz[j], e, p.c, p.fn, &act[j]);
+        if (p.offsets) trx[j] = __dadd_rn(trx[j], p.offsets[config * p.nc + ch]);
         act[j] = act[j] && pv[j];
       }
       for (int a = 0; a < p.na && ok; ++a) {

@@ -1024,6 +1024,41 @@ rcabeam_status rcabeam_opw_offsets_forward_device(const void* rc, const void* cr
   return launch_status();
 }
 
+rcabeam_status rcabeam_opw_offsets_power_device(const void* rc, const void* cr, const float* scan, const float* xe,
+                                                const float* ye, const float* angles, const float* starts,
+                                                const double* offsets, double c, float fs, float fd, float fn,
+                                                size_t ns, size_t nc, size_t na, size_t nt, size_t nv, float* pd,
+                                                void* workspace, size_t workspace_bytes) {
+  if (!rc || !cr || !scan || !xe || !ye || !angles || !starts || !offsets || !pd || !workspace || ns < 2 || !nc ||
+      !na || !nt || !nv || !(c > 0) || !(fs > 0) || !std::isfinite(c) || !std::isfinite(fs) || !std::isfinite(fd) ||
+      !std::isfinite(fn) || ns > INT32_MAX || nc > INT32_MAX || na > 4096 || nt > INT32_MAX || nv > INT32_MAX ||
+      nc * na > INT32_MAX)
+    return RCABEAM_ERROR_ARGUMENT;
+  if (cudaMemsetAsync(pd, 0, 2 * nv * sizeof(float), 0) != cudaSuccess) return RCABEAM_ERROR_CUDA;
+  das::Args a{};
+  a.rc = rc;
+  a.cr = cr;
+  a.scan = scan;
+  a.xe = xe;
+  a.ye = ye;
+  a.angles = angles;
+  a.starts = starts;
+  a.pd = pd;
+  a.ns = int(ns);
+  a.nc = int(nc);
+  a.na = int(na);
+  a.nt = int(nt);
+  a.nv = int(nv);
+  a.c = c;
+  a.fs = double(fs);
+  a.fd = double(fd);
+  a.fn = double(fn);
+  a.err = device_error_ptr();
+  a.offsets = offsets;
+  a.order = voxel_order(scan, nv, workspace, workspace_bytes);
+  return run_staged<false, das::kOpw>(a, (nv + das::kTileVoxels - 1) / das::kTileVoxels);
+}
+
 rcabeam_status rcabeam_opw_offsets_adjoint_device(const void* rc, const void* cr, const float* scan,
                                                   const unsigned* voxels, size_t nvl, const float* xe,
                                                   const float* ye, const float* angles, const float* starts,
