@@ -7,8 +7,9 @@
 //     pipeline -- the producer warp stages the tile's windows with TMA through
 //     the CTA's ring while the eight consumer warps interpolate (the same
 //     device functions as the single-ensemble staged kernel);
-//   * DMAS-CCF-ACF: blocks of kDmasVoxels voxels x 128 frames, one voxel per
-//     warp at a time (the same device function as the single-ensemble kernel).
+//   * DMAS-CCF-ACF: (64-voxel tile, 32-frame chunk) items of the same staged
+//     pipeline in two passes (channel-major, then angle-major), the device
+//     functions of the single-ensemble DMAS kernel.
 // Persistent CTAs take items from a global counter, so small and large
 // ensembles share the GPU without launch gaps or tails.  XDoppler magnitudes are
 // finished per tile by the CTA that completes the tile's last frame chunk, and
@@ -24,7 +25,7 @@
 namespace rcb {
 namespace batch {
 
-constexpr int kDmasVoxels = 4 * das::kConsumerWarps + 4;  // 36: four voxels per warp (nine warps)
+constexpr int kDmasLpv = 16;  // DMAS items: 32-frame chunks
 constexpr int kMaxAngles = 64;
 
 struct Ensemble {
@@ -59,7 +60,8 @@ struct Smem {
   static constexpr size_t kFull = kMeta + 64;
   static constexpr size_t kEmpty = kFull + 8 * das::kStages;
   static constexpr size_t kVox = kEmpty + 8 * das::kStages;
-  static constexpr size_t kItem = kVox + 4 * das::kTileVoxels;
+  static constexpr size_t kActive = kVox + 4 * das::kTileVoxels;  // DMAS: active channels per voxel
+  static constexpr size_t kItem = kActive + 4 * das::kTileVoxels;
   static constexpr size_t kAngles = kItem + 64;
   static constexpr size_t kBytes = kAngles + size_t(kMaxAngles) * 3 * sizeof(double);
 };
@@ -77,6 +79,20 @@ __device__ __forceinline__ bool staged(const Queue& q, const Ensemble& e, int ei
   return das::consume_item<LPV, false, das::kOpw>(e.args, vox, ring, frame0, warp, k);
 }
 
+// DMAS-CCF-ACF item: 64-voxel tile x 32-frame chunk, both passes through the ring.
+__device__ __forceinline__ bool staged_dmas(const Queue& q, const Ensemble& e, int ei, const das::Ring& ring,
+                                            const unsigned* vox, float* active, const double* angle_tab, int frame0,
+                                            uint32_t& k) {
+  const int warp = threadIdx.x >> 5;
+  if (warp == das::kConsumerWarps) {
+    const CUtensorMap* mr = q.maps + 2 * ei;
+    if (e.tma)
+      return das::produce_dmas_item<kDmasLpv, true>(mr, mr + 1, e.args, vox, angle_tab, ring, frame0, k, active);
+    return das::produce_dmas_item<kDmasLpv, false>(mr, mr + 1, e.args, vox, angle_tab, ring, frame0, k, active);
+  }
+  return das::consume_dmas_item<kDmasLpv>(e.args, vox, active, ring, frame0, warp, k);
+}
+
 // MINB resident CTAs per SM (register budget 65536 / (288 MINB)); the
 // autotuner picks the variant.
 template <int MINB>
@@ -89,6 +105,7 @@ __global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q) {
   long long* item_slot = reinterpret_cast<long long*>(smem + Smem::kItem);
   int* ens_slot = reinterpret_cast<int*>(smem + Smem::kItem + 8);
   int* fail = reinterpret_cast<int*>(smem + Smem::kItem + 12);
+  float* active = reinterpret_cast<float*>(smem + Smem::kActive);
   double* angle_tab = reinterpret_cast<double*>(smem + Smem::kAngles);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -125,22 +142,20 @@ __global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q) {
     const long long local = item - e.first_item;
     const int tile = int(local / e.chunks), chunk = int(local % e.chunks);
     bool ok = true;
-    if (e.method == 3) {
-      // DMAS-CCF-ACF: voxels [tile * kDmasVoxels, ...) of the 128-frame block `chunk`.
-      for (int j = warp; j < kDmasVoxels; j += das::kThreads / 32) {
-        const size_t v = size_t(tile) * kDmasVoxels + j;
-        if (v < size_t(e.args.nv)) generic::nonlinear_voxel<3>(e.args, v, chunk);
-      }
-    } else {
+    {
       das::load_item_tables(e.args, size_t(tile) * das::kTileVoxels, vox, angle_tab);
       __syncthreads();
       das::Ring r = ring;
       r.slot_bytes = size_t(das::kRows) * (2 * e.lpv) * 8;
       const int frame0 = chunk * 2 * e.lpv;
-      switch (e.lpv) {
-        case 8: ok = staged<8>(q, e, ei, r, vox, angle_tab, frame0, k); break;
-        case 16: ok = staged<16>(q, e, ei, r, vox, angle_tab, frame0, k); break;
-        default: ok = staged<32>(q, e, ei, r, vox, angle_tab, frame0, k); break;
+      if (e.method == 3) {
+        ok = staged_dmas(q, e, ei, r, vox, active, angle_tab, frame0, k);
+      } else {
+        switch (e.lpv) {
+          case 8: ok = staged<8>(q, e, ei, r, vox, angle_tab, frame0, k); break;
+          case 16: ok = staged<16>(q, e, ei, r, vox, angle_tab, frame0, k); break;
+          default: ok = staged<32>(q, e, ei, r, vox, angle_tab, frame0, k); break;
+        }
       }
     }
     if (!ok && lane == 0) atomicExch(fail, 1);

@@ -243,6 +243,26 @@ static rcabeam_status run_staged(das::Args a, size_t ntiles) {
   return RCABEAM_SUCCESS;
 }
 
+// DMAS-CCF-ACF on the staged pipeline: 32-frame chunks, both passes per CTA.
+static rcabeam_status run_dmas_staged(das::Args a, size_t ntiles) {
+  constexpr int kLpv = 16;
+  using S = das::Shape<kLpv, false>;
+  const size_t nt = size_t(a.nt);
+  const bool aligned = (nt * 8) % 16 == 0 && reinterpret_cast<uintptr_t>(a.rc) % 16 == 0 &&
+                       reinterpret_cast<uintptr_t>(a.cr) % 16 == 0 && encode_fn() != nullptr;
+  CUtensorMap mr{}, mq{};
+  const size_t slabs = size_t(a.nc) * a.na;
+  const bool tma = aligned && make_slab_map(&mr, a.rc, 8, nt, size_t(a.ns), slabs, S::kFrames, das::kRows) &&
+                   make_slab_map(&mq, a.cr, 8, nt, size_t(a.ns), slabs, S::kFrames, das::kRows);
+  const dim3 grid(unsigned(ntiles), unsigned((nt + S::kFrames - 1) / S::kFrames));
+  const size_t smem = S::bytes(a.na);
+  auto kern = tma ? das::dmas_staged<kLpv, true> : das::dmas_staged<kLpv, false>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+    return RCABEAM_ERROR_CUDA;
+  kern<<<grid, das::kThreads, smem>>>(mr, mq, a);
+  return launch_status();
+}
+
 static bool tc_eligible(const void* const* planes, int count, size_t nt) {
   if (nt % 4 != 0 || !encode_fn()) return false;
   for (int i = 0; i < count; ++i)
@@ -360,17 +380,15 @@ static rcabeam_status ensemble_impl(const void* rc, const void* cr, const float*
   a.fd = double(fd);
   a.fn = double(fn);
   a.err = device_error_ptr();
-  if (method == 2 || method == 3) {
+  if (method == 2) {
     dim3 grid(unsigned((nv + generic::kWarps - 1) / generic::kWarps),
               unsigned((nt + 32 * generic::kRegFrames - 1) / (32 * generic::kRegFrames)));
-    if (method == 2)
-      generic::ensemble_nonlinear<2><<<grid, generic::kWarps * 32>>>(a);
-    else
-      generic::ensemble_nonlinear<3><<<grid, generic::kWarps * 32>>>(a);
+    generic::ensemble_nonlinear<2><<<grid, generic::kWarps * 32>>>(a);
     return launch_status();
   }
   // The caller owns 2 * nv * (nc + na) float4 of scratch (reference rcabeam.h:196).
   a.order = voxel_order(scan, nv, geometry_workspace, 2 * nv * (nc + na) * 16);
+  if (method == 3) return run_dmas_staged(a, (nv + das::kTileVoxels - 1) / das::kTileVoxels);
   const size_t ntiles = (nv + das::kTileVoxels - 1) / das::kTileVoxels;
   const void* planes[2] = {rc, cr};
   if (HALF && tc_eligible(planes, 2, nt) && nv <= size_t(INT32_MAX) - tc::kVox && tc_smem_bytes(false, nt, na)) {
@@ -541,17 +559,15 @@ static rcabeam_status ensemble_static(const void* rc, const void* cr, const floa
   a.fd = double(fd);
   a.fn = double(fn);
   a.err = device_error_ptr();
-  if (method == 2 || method == 3) {
+  if (method == 2) {
     dim3 grid(unsigned((nv + generic::kWarps - 1) / generic::kWarps),
               unsigned((nt + 32 * generic::kRegFrames - 1) / (32 * generic::kRegFrames)));
-    if (method == 2)
-      generic::ensemble_nonlinear<2><<<grid, generic::kWarps * 32>>>(a);
-    else
-      generic::ensemble_nonlinear<3><<<grid, generic::kWarps * 32>>>(a);
+    generic::ensemble_nonlinear<2><<<grid, generic::kWarps * 32>>>(a);
     return launch_status();
   }
   // The sort rewrites keys, values and the bounding box (cleared inside) on every call.
   a.order = voxel_order(scan, nv, scratch, kStaticScratchBytes);
+  if (method == 3) return run_dmas_staged(a, (nv + das::kTileVoxels - 1) / das::kTileVoxels);
   const size_t ntiles = (nv + das::kTileVoxels - 1) / das::kTileVoxels;
   rcabeam_status st = method == 0   ? run_staged<false, das::kOpw>(a, ntiles)
                       : method == 5 ? run_staged<false, das::kApertures>(a, ntiles)
@@ -1109,8 +1125,9 @@ bool batch_plan(size_t n, const rcabeam_batch_ensemble* list, std::vector<batch:
     e.method = d.method;
     e.lpv = fpc / 2;
     if (d.method == 3) {
-      e.tiles = int((d.nv + batch::kDmasVoxels - 1) / batch::kDmasVoxels);
-      e.chunks = int((d.nt + 127) / 128);
+      e.lpv = batch::kDmasLpv;
+      e.tiles = int((d.nv + das::kTileVoxels - 1) / das::kTileVoxels);
+      e.chunks = int((d.nt + 2 * batch::kDmasLpv - 1) / (2 * batch::kDmasLpv));
     } else {
       e.tiles = int((d.nv + das::kTileVoxels - 1) / das::kTileVoxels);
       e.chunks = int((d.nt + fpc - 1) / fpc);
@@ -1192,7 +1209,7 @@ rcabeam_status rcabeam_batch_prepare(size_t n, const rcabeam_batch_ensemble* lis
   std::vector<CUtensorMap> maps(2 * n);
   for (size_t i = 0; i < n; ++i) {
     batch::Ensemble& e = ens[i];
-    if (e.method == 3 || !e.tma) continue;
+    if (!e.tma) continue;
     const int frames = 2 * e.lpv;
     const size_t slabs = size_t(e.args.nc) * e.args.na;
     if (!make_slab_map(&maps[2 * i], e.args.rc, 8, size_t(e.args.nt), size_t(e.args.ns), slabs, frames, das::kRows) ||
