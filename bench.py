@@ -302,7 +302,9 @@ def run_batching(args) -> dict:
         na = int(rng.choice([5, 7, 11]))
         chans = [torch.randn((ns * nc * na * nt,), dtype=torch.complex64, generator=gen, device=dev)
                  for _ in range(2)]
-        grid = (np.linspace(-half, half, 128), 4e-3 + dz * np.arange(depth), np.linspace(-half, half, 128))
+        lat = args.lateral
+        grid = (np.linspace(-half, half, 128)[(128 - lat) // 2:(128 + lat) // 2], 4e-3 + dz * np.arange(depth),
+                np.linspace(-half, half, 128)[(128 - lat) // 2:(128 + lat) // 2])
         e = batching.Ensemble(chans[0], chans[1], (ns, nc, na, nt), grid, geom,
                               np.deg2rad(np.linspace(-10, 10, na)), T_START, methods[i])
         e.build(dev)
@@ -354,8 +356,9 @@ def run_batching(args) -> dict:
         "latency_definition": "completion time since the queue started (device global timer for the persistent "
                               "kernel, CUDA events for sequential launches)",
         "dtype": "f32 math on c64 packed IQ (float64 geometry)", "data": "synthetic seeded complex Gaussian channels",
-        "config": {"workload": "48 ensembles: depth {128,192,256,384} at 128 x depth x 128, frames {50,100,200,400}, "
-                               "128 ch, angles {5,7,11}, ns 512, 50% OPW / 25% XDoppler / 25% DMAS-CCF-ACF",
+        "config": {"workload": f"{n} ensembles: depth {{128,192,256,384}} at {args.lateral} x depth x {args.lateral} "
+                               "(central block of the 128-wide grid), frames {50,100,200,400}, 128 ch, "
+                               "angles {5,7,11}, ns 512, 50% OPW / 25% XDoppler / 25% DMAS-CCF-ACF",
                    "seed": args.seed, "ensembles": shapes},
         "clocks": clocks, "gpu_launches": steps,
     }
@@ -606,6 +609,8 @@ def main() -> None:
     ap.add_argument("--casorati-frames", type=int, default=400, help="Casorati frames of the precision form")
     ap.add_argument("--ensembles", type=int, default=48, help="queue length of the batching form")
     ap.add_argument("--seed", type=int, default=5, help="seed of the batching queue")
+    ap.add_argument("--lateral", type=int, default=128,
+                    help="lateral x / y points of the batching queue's grids (central block of 128)")
     args = ap.parse_args()
     if args.form != "filtered":
         if args.impl == "b200" and int(os.environ.get("RANK", "0")) == 0:

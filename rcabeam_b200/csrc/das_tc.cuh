@@ -23,19 +23,21 @@
 // planes; with BF16 hi/lo coefficients each step runs three products
 // (Ahi Xhi + Alo Xhi + Ahi Xlo).  Accumulation is float32 in TMEM.
 //
-// Roles (288 threads, one CTA per SM, persistent over (tile, frame pass)):
-//   warps 0-3   builders.  A warp owns whole steps: channels are dealt round
-//               robin to the warps, so each warp forms the float64 receive
-//               delay and phase of its channel once for the 128 voxels (four
-//               per lane) and then, per angle, the taps (sample index, weight,
-//               phase by angle addition with a per-tile table of transmit
-//               delays and phases), the tile's row window (warp reductions),
-//               the A hi/lo rows of both groups, claims the next ring stage
-//               from a shared counter and stages the window with TMA
-//               (64-column x 16-row SWIZZLE_128B boxes, spread over lanes);
-//   warp 4      TMEM allocator; lane 0 issues tcgen05.mma and commits;
-//   warps 5-8   epilogue: tcgen05.ld of both accumulators, complex combine,
-//               IQ store and power.
+// Roles (one CTA per SM, persistent over (tile, frame pass)), with S ring
+// stages (the deepest of 5, 4, 3, 2 that fits shared memory):
+//   warps 0..S-1  builders, one per ring stage.  A warp owns whole steps:
+//               channels are dealt round robin to the warps, so each warp
+//               forms the float64 receive delay and phase of its channel once
+//               for the 128 voxels (four per lane) and then, per angle, the
+//               taps (sample index, weight, phase by angle addition with a
+//               per-tile table of transmit delays and phases), the tile's row
+//               window (warp reductions), the A hi/lo rows of both groups,
+//               claims the next ring stage from a shared counter and stages
+//               the window with TMA (64-column x 16-row SWIZZLE_128B boxes,
+//               spread over lanes);
+//   warp S      TMEM allocator; lane 0 issues tcgen05.mma and commits;
+//   warps S+1.. 4 epilogue warps: tcgen05.ld of both accumulators, complex
+//               combine, segment sums, IQ store and power.
 // Shared-memory operands: A is K-major without swizzle (8 x 16-byte core
 // matrices; LBO = 128 B between the two K cores, SBO = 256 B between 8-row
 // groups); X is MN-major SWIZZLE_128B straight from TMA (8-row x 128-byte
@@ -53,19 +55,18 @@ namespace tc {
 constexpr int kVox = 128;          // voxels per tile
 constexpr int kGroupVox = 64;      // voxels per M=128 MMA block
 constexpr int kRows = 16;
-constexpr int kStages = 4;         // ring depth when five stages do not fit shared memory
-constexpr int kDeepStages = 5;     // ring depth otherwise (decouples builders from the MMA)
+constexpr int kStages = 4;         // default ring depth for shared-memory estimates
+constexpr int kDeepStages = 5;     // deepest ring (the launcher takes the deepest of 5..2 that fits)
 constexpr int kBoxCols = 64;       // 16-bit columns per TMA box (one 128-byte swizzle atom)
 constexpr int kBoxBytes = kBoxCols * 2 * kRows;  // 2048
 constexpr int kMaxFrames = 128;    // frames per pass: 2 x frames columns <= 256 per group
-constexpr int kBuilders = 4;       // builder warps
-constexpr int kMmaWarp = kBuilders;
-constexpr int kThreads = (kBuilders + 1 + 4) * 32;
+// Warps: one builder per ring stage, then the MMA warp, then 4 epilogue warps.
+__host__ __device__ constexpr int threads_for(int stages) { return (stages + 1 + 4) * 32; }
 constexpr int kTmemCols = 512;     // group g accumulates in columns [256 g, 256 g + 2F)
 // Builders claim ring positions from a shared counter and wait for a stage by
 // mbarrier parity, which is unambiguous only while a waiter is at most one
 // phase ahead: that holds when no more builders than stages hold claims.
-static_assert(kBuilders <= kStages && kStages <= kDeepStages, "every builder needs its own ring stage");
+static_assert(kStages <= kDeepStages, "the deep ring is the larger one");
 constexpr int kAMatBytes = 128 * kRows * 2;  // 4096: one 128 x 16 16-bit matrix
 // FP16 coefficients (|c| <= 1) are scaled by 2^10 before the hi/lo split so that
 // the lo halves of small coefficients stay out of the FP16 subnormal range; the
@@ -226,10 +227,12 @@ __device__ __forceinline__ float2 demod_phase(double fd, double tau) {
 }
 
 template <bool BF16X3, int STAGES>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(threads_for(STAGES), 1)
     opw_tc(const __grid_constant__ CUtensorMap map_rc_hi, const __grid_constant__ CUtensorMap map_cr_hi,
            const __grid_constant__ CUtensorMap map_rc_lo, const __grid_constant__ CUtensorMap map_cr_lo, Args p) {
-  static_assert(kBuilders <= STAGES, "every builder needs its own ring stage");
+  // One builder warp per ring stage (builders may not outnumber stages).
+  constexpr int kBuilders = STAGES;
+  constexpr int kMmaWarp = kBuilders;
   using L = Layout<BF16X3>;
   constexpr int kPlanes = L::kPlanes;
   constexpr int kProducts = BF16X3 ? 3 : 2;

@@ -304,8 +304,11 @@ static float2* tc_partials_address() {
 template <bool BF16X3>
 static rcabeam_status run_tc(tc::Args a) {
   const size_t nt = size_t(a.nt);
-  const size_t deep = tc_smem_bytes(BF16X3, nt, size_t(a.na), tc::kDeepStages);
-  const size_t smem = deep ? deep : tc_smem_bytes(BF16X3, nt, size_t(a.na));
+  // The deepest ring (one builder warp per stage) that fits shared memory.
+  int stages = tc::kDeepStages;
+  size_t smem = 0;
+  for (; stages >= 2; --stages)
+    if ((smem = tc_smem_bytes(BF16X3, nt, size_t(a.na), stages))) break;
   if (!smem) return RCABEAM_ERROR_ARGUMENT;
   a.chunks = int((nt + tc::kMaxFrames - 1) / tc::kMaxFrames);
   int frames = int((nt + a.chunks - 1) / a.chunks);
@@ -327,14 +330,17 @@ static rcabeam_status run_tc(tc::Args a) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  auto kern = deep ? tc::opw_tc<BF16X3, tc::kDeepStages> : tc::opw_tc<BF16X3, tc::kStages>;
+  auto kern = stages == 5 ? tc::opw_tc<BF16X3, 5>
+              : stages == 4 ? tc::opw_tc<BF16X3, 4>
+              : stages == 3 ? tc::opw_tc<BF16X3, 3>
+                            : tc::opw_tc<BF16X3, 2>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
     return RCABEAM_ERROR_CUDA;
   a.partial = tc_partials_address();
   if (!a.partial) return RCABEAM_ERROR_CUDA;
   const int items = a.ntiles * a.chunks;
   const unsigned grid = unsigned(std::min(std::min(items, sms), tc::kMaxCtas));
-  kern<<<grid, tc::kThreads, smem>>>(mh[0], mh[1], ml[0], ml[1], a);
+  kern<<<grid, tc::threads_for(stages), smem>>>(mh[0], mh[1], ml[0], ml[1], a);
   return launch_status();
 }
 
@@ -391,7 +397,7 @@ static rcabeam_status ensemble_impl(const void* rc, const void* cr, const float*
   if (method == 3) return run_dmas_staged(a, (nv + das::kTileVoxels - 1) / das::kTileVoxels);
   const size_t ntiles = (nv + das::kTileVoxels - 1) / das::kTileVoxels;
   const void* planes[2] = {rc, cr};
-  if (HALF && tc_eligible(planes, 2, nt) && nv <= size_t(INT32_MAX) - tc::kVox && tc_smem_bytes(false, nt, na)) {
+  if (HALF && tc_eligible(planes, 2, nt) && nv <= size_t(INT32_MAX) - tc::kVox && tc_smem_bytes(false, nt, na, 2)) {
     tc::Args t{};
     t.x_hi[0] = rc;
     t.x_hi[1] = cr;

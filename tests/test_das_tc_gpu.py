@@ -93,3 +93,18 @@ def test_tc_long_line_and_empty_tiles():
     # Voxels with no valid tap are exact zeros in both.
     dead = np.all(expected == 0, axis=-1)
     assert np.all(actual[dead] == 0)
+
+
+@pytest.mark.parametrize("storage", ["float16", "bf16x2"])
+@pytest.mark.parametrize("angles", [15, 24])
+def test_tc_many_angles_shallow_ring(storage, angles):
+    """200 frames with 15 angles still fits the five-stage ring (five builders); with 24 angles the
+    per-tile transmit tables leave room for a three-stage ring (three builders)."""
+    grid = (np.linspace(-1e-3, 1e-3, 6), np.linspace(3e-3, 6e-3, 7), np.linspace(-1e-3, 1e-3, 5))
+    rc, cr, _, starts, grid, geom = random_case(31, 96, 8, angles, 200, grid, fnumber=None, fs=20e6, fd=15e6,
+                                                starts=np.full(angles, 2e-6))
+    ang = np.deg2rad(np.linspace(-10, 10, angles))
+    ref_in = (_quant(rc), _quant(cr)) if storage == "float16" else (rc, cr)
+    expected = _oracle(*ref_in, ang, starts, grid, geom).reshape(6, 7, 5, 200)
+    actual = rb.beamform_ensemble(rc, cr, ang, starts, grid, geom, iq_storage=storage)
+    assert rel_l2(actual, expected) <= 5e-5
