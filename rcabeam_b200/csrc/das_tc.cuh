@@ -24,7 +24,8 @@
 // (Ahi Xhi + Alo Xhi + Ahi Xlo).  Accumulation is float32 in TMEM.
 //
 // Roles (one CTA per SM, persistent over (tile, frame pass)), with S ring
-// stages (the deepest of 5, 4, 3, 2 that fits shared memory):
+// stages (the deepest of 6..2 that fits shared memory; 352 threads x 168
+// registers at six stages still fit the register file):
 //   warps 0..S-1  builders, one per ring stage.  A warp owns whole steps:
 //               channels are dealt round robin to the warps, so each warp
 //               forms the float64 receive delay and phase of its channel once
@@ -56,7 +57,7 @@ constexpr int kVox = 128;          // voxels per tile
 constexpr int kGroupVox = 64;      // voxels per M=128 MMA block
 constexpr int kRows = 16;
 constexpr int kStages = 4;         // default ring depth for shared-memory estimates
-constexpr int kDeepStages = 5;     // deepest ring (the launcher takes the deepest of 5..2 that fits)
+constexpr int kDeepStages = 6;     // deepest ring (the launcher takes the deepest of 6..2 that fits)
 constexpr int kBoxCols = 64;       // 16-bit columns per TMA box (one 128-byte swizzle atom)
 constexpr int kBoxBytes = kBoxCols * 2 * kRows;  // 2048
 constexpr int kMaxFrames = 128;    // frames per pass: 2 x frames columns <= 256 per group

@@ -330,7 +330,8 @@ static rcabeam_status run_tc(tc::Args a) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  auto kern = stages == 5 ? tc::opw_tc<BF16X3, 5>
+  auto kern = stages == 6 ? tc::opw_tc<BF16X3, 6>
+              : stages == 5 ? tc::opw_tc<BF16X3, 5>
               : stages == 4 ? tc::opw_tc<BF16X3, 4>
               : stages == 3 ? tc::opw_tc<BF16X3, 3>
                             : tc::opw_tc<BF16X3, 2>;
