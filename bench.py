@@ -43,8 +43,9 @@ FS, FD, C = 20e6, 15e6, 1540.0
 T_START = 4e-6
 RANK_START = 3
 # DRAM bytes (read + write) per unit of the bf16x3 tensor-core DAS launch,
-# from one ncu capture: 1012.2 MB for 65,536 voxels x 256 ch x 11 ang x 104 frm.
-DAS_DRAM_BYTES_PER_UNIT = 1012.19e6 / (65536 * 256 * 11 * 104)
+# from one ncu capture: 1609.3 MB for 65,536 voxels x 256 ch x 11 ang x 104 frm
+# (the 512-step segment partial sums account for most of the writes).
+DAS_DRAM_BYTES_PER_UNIT = 1609.26e6 / (65536 * 256 * 11 * 104)
 
 
 SUBGRID = None  # (nx, nz, ny) central block of the full grid, same spacing (profiling)
