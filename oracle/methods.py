@@ -2,6 +2,11 @@
 
 * XDoppler, method 1: |mean_t r_t conj(q_t)| with r, q the RC and CR
   compounded IQ (src/rcabeam/xdoppler.py:33-51; ensemble.cu:236-315, 596-627).
+* St-SW, method 4: interleaved angle subsets s::k of each aperture, per-frame
+  subset means and variances, the k x k cross-correlation series, their
+  energies over frames and the normalized pair sum, times XDoppler power
+  (src/rcabeam/stsw.py:10-107; the C ABI returns the raw weights and the
+  caller normalizes by the full-volume peak, ensemble.py:127-129).
 * DMAS-CCF-ACF, method 3: per frame, signed-square-root channel DMAS, the
   cross-coherence factor over active channels and the angular coherence factor,
   then the mean over frames (src/rcabeam/dmas.py:32-85 evaluated on per-frame
@@ -88,3 +93,57 @@ def dmas_ccf_acf_power(rc, cr, scan, xe, ye, angles, starts, c, fs, fd, fnumber)
     w_ccf = np.where(np.isfinite(w_ccf), w_ccf, 0)
     w_acf = np.where(np.isfinite(w_acf) & (den > 0), w_acf, 0)
     return np.mean(y_dmas * w_ccf * w_acf, axis=-1)
+
+
+def _subset_stats(per_angle: np.ndarray, k: int):
+    """Means and mean squared deviations over angles s::k, per frame (stsw.py:45-53)."""
+    means, variances = [], []
+    for subset in range(k):
+        group = per_angle[:, subset::k, :]
+        mu = group.mean(axis=1)
+        means.append(mu)
+        variances.append(np.mean(np.abs(group - mu[:, None, :]) ** 2, axis=1))
+    return means, variances
+
+
+def st_sw_raw_weights(per_angle_rc: np.ndarray, per_angle_cr: np.ndarray, k: int) -> np.ndarray:
+    """Unnormalized St-SW weights ``|acc|`` per voxel from per-angle IQ ``(nv, na, nt)`` (stsw.py:54-79)."""
+    m_rc, v_rc = _subset_stats(per_angle_rc, k)
+    m_cr, v_cr = _subset_stats(per_angle_cr, k)
+    ccf, energy = {}, {}
+    for ir in range(k):
+        for ic in range(k):
+            num = m_rc[ir] * np.conj(m_cr[ic])
+            den = np.abs(m_rc[ir]) ** 2 + np.abs(m_cr[ic]) ** 2 + (v_rc[ir] + v_cr[ic]) / 2 - np.abs(num)
+            with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+                value = num / den
+            value[~np.isfinite(value)] = 0
+            ccf[ir, ic] = value
+            energy[ir, ic] = np.sum(np.abs(value) ** 2, axis=-1)
+    acc = np.zeros(per_angle_rc.shape[0], dtype=np.complex128)
+    for ir1 in range(k):
+        for ic1 in range(k):
+            for ir2 in range(ir1 + 1, k):
+                for ic2 in range(k):
+                    if ic2 == ic1:
+                        continue
+                    den = np.sqrt(energy[ir1, ic1] * energy[ir2, ic2])
+                    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+                        corr = np.sum(ccf[ir1, ic1] * np.conj(ccf[ir2, ic2]), axis=-1) / den
+                    corr[~np.isfinite(corr)] = 0
+                    acc += corr
+    return np.abs(acc)
+
+
+def st_sw_terms(rc, cr, scan, xe, ye, angles, starts, c, fs, fd, fnumber, k):
+    """(raw weights, XDoppler power) per voxel: the two outputs of C ABI method 4."""
+    _, ar, _ = aperture_terms(rc, scan, xe, angles, starts, c, fs, fd, fnumber, "RC")
+    _, aq, _ = aperture_terms(cr, scan, ye, angles, starts, c, fs, fd, fnumber, "CR")
+    return st_sw_raw_weights(ar, aq, k), xdoppler_power(ar.sum(axis=1), aq.sum(axis=1))
+
+
+def st_sw_power(rc, cr, scan, xe, ye, angles, starts, c, fs, fd, fnumber, k):
+    """St-SW power Doppler: peak-normalized weights times XDoppler power (stsw.py:82-107)."""
+    weights, power = st_sw_terms(rc, cr, scan, xe, ye, angles, starts, c, fs, fd, fnumber, k)
+    peak = weights.max()
+    return (weights / peak if peak > 0 else weights) * power

@@ -5,7 +5,7 @@ Run in a container where the reference checkout is available:
     python tests/golden/make_golden.py /path/to/rcabeam
 
 It imports ``rcabeam`` from ``<reference>/src`` (NumPy modules only: sim,
-clutter, power, opw, ensemble.opw_voxel_order, dmas, fmas) and writes
+clutter, power, opw, ensemble.opw_voxel_order, dmas, fmas, stsw) and writes
 ``tests/golden/*.npz``.  The fixtures hold the exact inputs next to the
 reference outputs, so the tests never need the reference at run time.
 """
@@ -146,8 +146,49 @@ def dmas_cases(sim, dmas):
     return {"dmas_f1_power": np.mean(out, axis=0)}
 
 
+def stsw_cases(sim, stsw):
+    """St-SW power from per-frame per-angle DAS, as tests/test_ensemble.py:30-69 and
+    tests/test_ensemble_targets.py:46-65 build it (k = 2, 3, 4)."""
+    cases = {}
+    # Small case of test_ensemble.py (full aperture, 5 frames).
+    rng = np.random.default_rng(44)
+    geom = sim.RCAGeometry(x_el=np.array([-0.001, 0.001]), y_el=np.array([-0.0008, 0.0007]), fs=1e6, f_demod=0.1e6)
+    angles = np.array([-0.08, -0.02, 0.05, 0.09])
+    starts = np.array([1e-6, 2e-6, 1e-6, 3e-6])
+    grid = (np.array([0.0, 0.008]), np.array([0.001, 0.007, 0.03]), np.array([0.0]))
+    rc = (rng.normal(size=(16, 2, 4, 5)) + 1j * rng.normal(size=(16, 2, 4, 5))).astype(np.complex64)
+    cr = (rng.normal(size=rc.shape) + 1j * rng.normal(size=rc.shape)).astype(np.complex64)
+    # A lateral line of 257 voxels, 3 frames, RC angle 0 silent (zero-norm series for k = 4).
+    line_grid = (np.zeros(1), np.array([0.007]), np.linspace(-0.001, 0.001, 257))
+    line_geom = sim.RCAGeometry(x_el=np.array([-0.001, 0.001]), y_el=np.array([-0.001, 0.001]), fs=1e6,
+                                f_demod=0.1e6)
+    rng = np.random.default_rng(42)
+    lr = (rng.normal(size=(16, 2, 4, 3)) + 1j * rng.normal(size=(16, 2, 4, 3))).astype(np.complex64)
+    lq = (rng.normal(size=lr.shape) + 1j * rng.normal(size=lr.shape)).astype(np.complex64)
+    lr[:, :, 0] = 0
+    for tag, (r, q, st, g, gm) in {"small": (rc, cr, starts, grid, geom),
+                                   "line": (lr, lq, 1e-6, line_grid, line_geom)}.items():
+        ar, aq = [], []
+        for t in range(r.shape[-1]):
+            _, a, _ = sim.delay_rca_channel_data(r[..., t], angles, st, g, gm, "RC", use_cuda=False)
+            _, b, _ = sim.delay_rca_channel_data(q[..., t], angles, st, g, gm, "CR", use_cuda=False)
+            ar.append(a)
+            aq.append(b)
+        iq = np.concatenate([np.stack(ar, axis=-1), np.stack(aq, axis=-1)], axis=-2)
+        ri, qi = np.arange(4), np.arange(4, 8)
+        for k in (2, 3, 4):
+            cases[f"{tag}_k{k}_power"] = stsw.st_sw_pd(iq, ri, qi, k=k)
+            cases[f"{tag}_k{k}_weights"] = stsw.st_sw_weights(iq, ri, qi, k=k)
+        cases[f"{tag}_rc"], cases[f"{tag}_cr"] = r, q
+    cases.update(angles=angles, small_starts=starts, line_y=line_grid[2])
+    return cases
+
+
 def main(root: str) -> None:
     sim, clutter, ensemble, dmas = _import_reference(root)
+    import rcabeam.stsw as stsw
+
+    np.savez_compressed(HERE / "stsw.npz", **stsw_cases(sim, stsw))
     np.savez_compressed(HERE / "das.npz", **das_cases(sim))
     np.savez_compressed(HERE / "clutter.npz", **clutter_cases(clutter))
     np.savez_compressed(HERE / "order.npz", **order_cases(ensemble))

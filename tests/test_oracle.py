@@ -105,3 +105,25 @@ def test_clutter_oracle_policy():
 def test_power_doppler_oracle():
     x = np.array([[1 + 1j, 2, 0, 1j]])
     np.testing.assert_allclose(das.power_doppler(x), [(2 + 4 + 0 + 1) / 4])
+
+
+@pytest.mark.parametrize("tag", ["small", "line"])
+@pytest.mark.parametrize("k", [2, 3, 4])
+def test_st_sw_oracle_matches_reference(tag, k):
+    """St-SW weights and power against the reference's st_sw_weights / st_sw_pd (stsw.py:10-107)."""
+    s = np.load(GOLDEN / "stsw.npz")
+    if tag == "small":
+        scan = _grid_scan([0.0, 0.008], [0.001, 0.007, 0.03], [0.0])
+        xe, ye, starts = np.array([-0.001, 0.001]), np.array([-0.0008, 0.0007]), s["small_starts"]
+    else:
+        scan = _grid_scan([0.0], [0.007], s["line_y"])
+        xe = ye = np.array([-0.001, 0.001])
+        starts = 1e-6
+    # The fixtures use RCAGeometry's default aperture, f-number 1 (sim.py:12-37).
+    args = (s[f"{tag}_rc"], s[f"{tag}_cr"], scan, xe, ye, s["angles"], starts, 1540.0, 1e6, 0.1e6, 1.0, k)
+    weights, _ = methods.st_sw_terms(*args)
+    ref_w = s[f"{tag}_k{k}_weights"].ravel()
+    peak = weights.max()
+    # The reference keeps per-angle IQ in complex64 (sim.py:344-393): agreement to its rounding.
+    np.testing.assert_allclose(weights / peak, ref_w, rtol=2e-6, atol=1e-6)
+    np.testing.assert_allclose(methods.st_sw_power(*args), s[f"{tag}_k{k}_power"].ravel(), rtol=2e-6, atol=1e-6)
