@@ -239,8 +239,9 @@ def run_b200(args, rank: int, world: int) -> dict | None:
     # M=128 x N=2*frames x K=16 MMA (sub-window splits excluded).
     tiles = (int(np.prod(SUBGRID or GRID_SHAPE)) + 127) // 128
     passes = (NT + 127) // 128
-    frames = ((NT + passes - 1) // passes + 7) // 8 * 8
-    mma_flops = tiles * passes * 2 * NC * NA * 2 * 3 * 2 * 128 * (2 * frames) * 16
+    full = 128 if NT > 128 else (NT + 7) // 8 * 8
+    pass_frames = [full] * (passes - 1) + [(NT - full * (passes - 1) + 7) // 8 * 8]
+    mma_flops = tiles * 2 * NC * NA * 2 * 3 * 2 * 128 * sum(2 * f for f in pass_frames) * 16
     # Compulsory HBM bytes of one DAS launch: hi+lo packed planes read, IQ + power written.
     nvox = int(np.prod(SUBGRID or GRID_SHAPE))
     das_bytes = 2 * NS * NC * NA * NT * 8 + nvox * NT * 8 + nvox * 8
@@ -263,8 +264,8 @@ def run_b200(args, rank: int, world: int) -> dict | None:
                                        "central 32x64x32 block (104 frames), scaled by units "
                                        "(profiles/opw_tc_bf16x3_central_block_ncu.md)",
                      "das_ms": ch["das_ms"],
-                     "note": "dense tcgen05 MMA flops issued per launch (2 groups x 3 products x M128 x N208 x K16 per "
-                             "128-voxel tile step) vs "
+                     "note": "dense tcgen05 MMA flops issued per launch (2 groups x 3 products x M128 x N(2 x pass "
+                             f"frames {pass_frames}) x K16 per 128-voxel tile step) vs "
                              "measured sustained bf16 peak (of measured); compulsory HBM bytes "
                              f"{das_bytes / 1e9:.2f} GB per launch -> {das_bytes / das_s / 1e9:.1f} GB/s"},
         "clocks": clock,

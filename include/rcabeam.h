@@ -122,7 +122,10 @@ rcabeam_status rcabeam_pack_ensemble_device(const void* source, void* target, si
  * complex64.  method: 0 OPW, 1 XDoppler, 2 RC-FMAS, 3 DMAS-CCF-ACF, 4 St-SW,
  * 5 separate RC/CR IQ.  pd: 2*nv floats, the result is in the even entries.
  * signal: optional complex64 (nv, nt) output ((nv, 2, nt) for method 5).
- * weights/workspace: St-SW only.  geometry_workspace: caller-owned scratch of
+ * weights/workspace: St-SW only: weights[nv] receives the raw St-SW weights
+ * (normalize by their full-volume maximum before multiplying pd), workspace is
+ * complex64 [nv * k * k * nt] correlation-series scratch, 2 <= k <= 4, na >= k,
+ * signal must be null.  geometry_workspace: caller-owned scratch of
  * 2*nv*(nc+na) float4; this implementation computes delays on the fly and uses
  * the scratch only for its voxel traversal order.  Delays and phases are formed
  * in float64; interpolation and accumulation are float32. */

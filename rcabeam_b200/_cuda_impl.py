@@ -19,6 +19,8 @@ import torch
 from rcabeam_b200 import _lib
 
 _COMPLEX64 = (np.complex64, torch.complex64)
+# Device scratch for the St-SW correlation series of one voxel tile.
+_STSW_SCRATCH_BYTES = 256 << 20
 
 
 def _ptr(t: torch.Tensor | None) -> int | None:
@@ -83,6 +85,10 @@ def ensemble_from_channels(rc, cr, scan, xe, ye, angles, starts, pd, signal, wei
         raise ValueError("FP16 IQ storage is supported only for OPW")
     if storage == "bf16x2" and nt % 4:
         raise ValueError("bf16x2 storage requires a frame count divisible by 4")
+    if method == 4 and (weights is None or len(weights) != nv):
+        raise ValueError("invalid ensemble output shapes")
+    if method == 4 and (k < 2 or k > 4 or na < k):
+        raise ValueError("St-SW needs 2<=k<=4 and at least k angles")
     host_in = not isinstance(rc, torch.Tensor) or not rc.is_cuda
     begin = time.perf_counter()
     d_rc = _to_device(rc, torch.complex64)
@@ -129,9 +135,26 @@ def ensemble_from_channels(rc, cr, scan, xe, ye, angles, starts, pd, signal, wei
                   lo_cr.data_ptr(), d_scan.data_ptr(), d_xe.data_ptr(), d_ye.data_ptr(), d_angles.data_ptr(),
                   d_starts.data_ptr(), d_pd.data_ptr(), _ptr(d_sig), geometry.data_ptr(), ns, nc, na, nt, nv, c, fs,
                   fd, fn, 1)
+    elif method == 4:
+        # St-SW keeps k^2 correlation series per voxel and frame: voxel tiles
+        # bound that scratch (reference python.cpp:553-565 tiles for the same reason).
+        for src, dst in ((d_rc, packed_rc), (d_cr, packed_cr)):
+            _lib.call("rcabeam_pack_ensemble_device", src.data_ptr(), dst.data_ptr(), ns, nc, na, nt)
+        tile = max(1, min(nv, _STSW_SCRATCH_BYTES // (k * k * nt * 8)))
+        series = torch.empty(tile * k * k * nt, dtype=torch.complex64, device=dev)
+        d_w = torch.empty(nv, dtype=torch.float32, device=dev)
+        for v0 in range(0, nv, tile):
+            count = min(tile, nv - v0)
+            _lib.call("rcabeam_ensemble_device", packed_rc.data_ptr(), packed_cr.data_ptr(),
+                      d_scan.data_ptr() + 12 * v0, d_xe.data_ptr(), d_ye.data_ptr(), d_angles.data_ptr(),
+                      d_starts.data_ptr(), d_pd.data_ptr() + 8 * v0, None, d_w.data_ptr() + 4 * v0,
+                      series.data_ptr(), geometry.data_ptr(), ns, nc, na, nt, count, c, fs, fd, fn, method, k)
+        if isinstance(weights, torch.Tensor) and weights.is_cuda:
+            weights.copy_(d_w)
+        else:
+            torch.cuda.synchronize()
+            np.copyto(np.asarray(weights).reshape(nv), d_w.cpu().numpy())
     else:
-        if method == 4:
-            raise ValueError("St-SW is not provided by this implementation")
         for src, dst in ((d_rc, packed_rc), (d_cr, packed_cr)):
             _lib.call("rcabeam_pack_ensemble_device", src.data_ptr(), dst.data_ptr(), ns, nc, na, nt)
         _lib.call("rcabeam_ensemble_device", packed_rc.data_ptr(), packed_cr.data_ptr(), d_scan.data_ptr(),
@@ -189,16 +212,17 @@ def opw_from_packed(rc, cr, scan, xe, ye, angles, starts, pd, signal, geometry_w
     nbytes = ns * nc * na * nt * (4 if half_storage else 8)
     if (rc.numel() != nbytes or cr.numel() != nbytes or xe.numel() != nc or ye.numel() != nc
             or angles.numel() != na or starts.numel() != na or pd.shape[0] != nv
-            or tuple(signal.shape) != (nv, nt) or geometry_workspace.numel() < workspace_bytes(nv, nc, na)):
+            or (signal is not None and tuple(signal.shape) != (nv, nt))
+            or geometry_workspace.numel() < workspace_bytes(nv, nc, na)):
         raise ValueError("invalid resident buffer shapes")
     fn_name = "rcabeam_opw_fp16_device" if half_storage else "rcabeam_ensemble_device"
     if half_storage:
         _lib.call(fn_name, rc.data_ptr(), cr.data_ptr(), scan.data_ptr(), xe.data_ptr(), ye.data_ptr(),
-                  angles.data_ptr(), starts.data_ptr(), pd.data_ptr(), signal.data_ptr(),
+                  angles.data_ptr(), starts.data_ptr(), pd.data_ptr(), _ptr(signal),
                   geometry_workspace.data_ptr(), ns, nc, na, nt, nv, c, fs, fd, fn)
     else:
         _lib.call(fn_name, rc.data_ptr(), cr.data_ptr(), scan.data_ptr(), xe.data_ptr(), ye.data_ptr(),
-                  angles.data_ptr(), starts.data_ptr(), pd.data_ptr(), signal.data_ptr(), None, None,
+                  angles.data_ptr(), starts.data_ptr(), pd.data_ptr(), _ptr(signal), None, None,
                   geometry_workspace.data_ptr(), ns, nc, na, nt, nv, c, fs, fd, fn, 0, 2)
     if synchronize:
         torch.cuda.synchronize()

@@ -197,6 +197,151 @@ __global__ void __launch_bounds__(kWarps * 32) ensemble_nonlinear(das::Args p) {
   nonlinear_voxel<METHOD>(p, v, blockIdx.y);
 }
 
+// ------------------------------------------------------------ St-SW --
+// St-SW (method 4; reference stsw.py:10-107, ensemble.cu:457-627).  Angles of
+// each aperture fall into K interleaved subsets (a % K).  Per frame: the
+// subset means m and mean squared deviations v of the per-angle sums, the
+// K x K series c[i][j] = m_rc[i] conj(m_cr[j]) / (|m_rc[i]|^2 + |m_cr[j]|^2 +
+// (v_rc[i] + v_cr[j]) / 2 - |m_rc[i] conj(m_cr[j])|); over frames the raw
+// weight |sum over (i1 < i2, j1 != j2) of sum_t c1 conj(c2) / sqrt(E1 E2)| with
+// E the series energies; the power is the XDoppler |mean_t r conj(q)|.
+//
+// Pass 1 (one warp per voxel, lanes over frames): per-angle channel sums in
+// angle-major order with the taps broadcast as for RC-FMAS, Welford updates of
+// the subset statistics (no E|x|^2 - |E x|^2 cancellation), the series written
+// to the caller's workspace (v K^2 + i K + j) nt + t and r conj(q) summed into
+// pd[2v], pd[2v + 1].
+template <int K, int RF>
+__global__ void __launch_bounds__(kWarps * 32) stsw_series(das::Args p, float2* series) {
+  const size_t v = size_t(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (v >= size_t(p.nv)) return;
+  const int lane = threadIdx.x & 31;
+  const int fbase = blockIdx.y * 32 * RF + lane;
+  const Voxel q = load_voxel(p.scan, v);
+  const float2* rc = static_cast<const float2*>(p.rc);
+  const float2* cr = static_cast<const float2*>(p.cr);
+  float2 r[RF] = {}, s[RF] = {};
+  float2 mr[K][RF] = {}, mq[K][RF] = {};
+  float vr[K][RF] = {}, vq[K][RF] = {};
+  for (int a = 0; a < p.na; ++a) {
+    float2 ar[RF] = {}, aq[RF] = {};
+    for (int c0 = 0; c0 < p.nc; c0 += 32) {
+      const Tap lr = lane_tap(p, q, 0, true, a, c0), lq = lane_tap(p, q, 1, true, a, c0);
+      const int count = min(32, p.nc - c0);
+      for (int j = 0; j < count; ++j) {
+        const int ch = c0 + j;
+        const Tap tr = shfl_tap(lr, j), tq = shfl_tap(lq, j);
+#pragma unroll
+        for (int f = 0; f < RF; ++f) {
+          const int frame = fbase + 32 * f;
+          ar[f] = cadd(ar[f], packed_sample(rc, tr, ch, a, frame, p.ns, p.na, p.nt));
+          aq[f] = cadd(aq[f], packed_sample(cr, tq, ch, a, frame, p.ns, p.na, p.nt));
+        }
+      }
+    }
+    // Welford update of subset a % K, whose (a / K + 1)-th angle this is.
+    const int subset = a % K;
+    const float inv = 1.0f / float(a / K + 1);
+#pragma unroll
+    for (int f = 0; f < RF; ++f) {
+      r[f] = cadd(r[f], ar[f]);
+      s[f] = cadd(s[f], aq[f]);
+#pragma unroll
+      for (int i = 0; i < K; ++i) {
+        if (i != subset) continue;
+        const float2 dr = make_float2(ar[f].x - mr[i][f].x, ar[f].y - mr[i][f].y);
+        const float2 dq = make_float2(aq[f].x - mq[i][f].x, aq[f].y - mq[i][f].y);
+        mr[i][f] = make_float2(fmaf(dr.x, inv, mr[i][f].x), fmaf(dr.y, inv, mr[i][f].y));
+        mq[i][f] = make_float2(fmaf(dq.x, inv, mq[i][f].x), fmaf(dq.y, inv, mq[i][f].y));
+        vr[i][f] += dr.x * (ar[f].x - mr[i][f].x) + dr.y * (ar[f].y - mr[i][f].y);
+        vq[i][f] += dq.x * (aq[f].x - mq[i][f].x) + dq.y * (aq[f].y - mq[i][f].y);
+      }
+    }
+  }
+  float cross_re = 0.f, cross_im = 0.f;
+#pragma unroll
+  for (int f = 0; f < RF; ++f) {
+    const int frame = fbase + 32 * f;
+    if (frame >= p.nt) continue;
+    const float2 x = cmul(r[f], cconj(s[f]));
+    cross_re += x.x;
+    cross_im += x.y;
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      // Subset i holds the angles i, i + K, ... < na.
+      const float count = float((p.na - 1 - i) / K + 1);
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        const float countq = float((p.na - 1 - j) / K + 1);
+        const float2 num = cmul(mr[i][f], cconj(mq[j][f]));
+        const float den = cabs2(mr[i][f]) + cabs2(mq[j][f]) + (vr[i][f] / count + vq[j][f] / countq) * 0.5f -
+                          hypotf(num.x, num.y);
+        float2 value = den > 0.f ? make_float2(num.x / den, num.y / den) : make_float2(0.f, 0.f);
+        if (!isfinite(value.x) || !isfinite(value.y)) value = make_float2(0.f, 0.f);
+        series[(v * (K * K) + size_t(i * K + j)) * size_t(p.nt) + size_t(frame)] = value;
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    cross_re += __shfl_xor_sync(0xffffffffu, cross_re, off);
+    cross_im += __shfl_xor_sync(0xffffffffu, cross_im, off);
+  }
+  if (lane == 0) {
+    atomicAdd(p.pd + 2 * v, cross_re / float(p.nt));
+    atomicAdd(p.pd + 2 * v + 1, cross_im / float(p.nt));
+  }
+}
+
+// Pass 2 (one warp per voxel): series energies over frames, then the pair sum
+// with running row / column sums of the normalized series (for row i, the
+// earlier rows' total minus their column j pairs with c[i][j]), the raw weight
+// |acc| and the XDoppler magnitude in pd[2v].
+template <int K>
+__global__ void __launch_bounds__(kWarps * 32) stsw_finish(float* pd, float* weights, const float2* series,
+                                                           size_t nv, int nt) {
+  const size_t v = size_t(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (v >= nv) return;
+  const int lane = threadIdx.x & 31;
+  const float2* base = series + v * (K * K) * size_t(nt);
+  float scale[K * K];
+#pragma unroll
+  for (int e = 0; e < K * K; ++e) {
+    float energy = 0.f;
+    for (int t = lane; t < nt; t += 32) energy += cabs2(base[size_t(e) * nt + t]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) energy += __shfl_xor_sync(0xffffffffu, energy, off);
+    scale[e] = energy > 0.f ? 1.0f / sqrtf(energy) : 0.f;
+  }
+  float2 acc = make_float2(0.f, 0.f);
+  for (int t = lane; t < nt; t += 32) {
+    float2 total = make_float2(0.f, 0.f), column[K] = {};
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      float2 row = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        const float2 raw = base[size_t(i * K + j) * nt + t];
+        const float2 value = make_float2(raw.x * scale[i * K + j], raw.y * scale[i * K + j]);
+        const float2 earlier = make_float2(total.x - column[j].x, total.y - column[j].y);
+        acc = cadd(acc, cmul(earlier, cconj(value)));
+        column[j] = cadd(column[j], value);
+        row = cadd(row, value);
+      }
+      total = cadd(total, row);
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+  }
+  if (lane == 0) {
+    weights[v] = hypotf(acc.x, acc.y);
+    pd[2 * v] = hypotf(pd[2 * v], pd[2 * v + 1]);
+  }
+}
+
 // --------------------------------------------- single-frame API (core.cu) --
 // Channel layout (samples, channels, angles); one frame.
 __device__ __forceinline__ float2 frame_sample(const float2* iq, const Voxel& q, const float* el, const float* angles,

@@ -15,7 +15,9 @@
 // and lane 2v + 1 holds Q = Im(A) X, and the voxel's IQ is
 // (P_re - Q_im) + j (P_im + Q_re).  Both 64-voxel groups of a tile use the
 // same staged window (two MMAs per product), which halves the window bytes
-// per interpolated sample; frames beyond 128 run as further passes.
+// per interpolated sample.  Frames run in passes of 128 (N = 256: four whole
+// 64-column TMA boxes per plane) and a last pass of the remainder rounded up
+// to 8 frames, so no staged column is wasted except in the last box.
 //
 // Precision: FP16-packed channels are exact FP16 and the coefficients are
 // split into FP16 hi + lo (two products, coefficients scaled by 2^10 so the lo
@@ -32,10 +34,12 @@
 //               for the 128 voxels (four per lane) and then, per angle, the
 //               taps (sample index, weight, phase by angle addition with a
 //               per-tile table of transmit delays and phases), the tile's row
-//               window (warp reductions), the A hi/lo rows of both groups,
-//               claims the next ring stage from a shared counter and stages
-//               the window with TMA (64-column x 16-row SWIZZLE_128B boxes,
-//               spread over lanes);
+//               window (warp reductions) and the hi / lo coefficient pairs;
+//               then claims the next ring stage from a shared counter, issues
+//               the window's TMA copies (64-column x 16-row SWIZZLE_128B boxes,
+//               spread over lanes) and, while they fly, writes the A rows of
+//               both groups from registers (bank-conflict-free 16-byte
+//               stores) before its 32 arrivals on the stage's barrier;
 //   warp S      TMEM allocator; lane 0 issues tcgen05.mma and commits;
 //   warps S+1.. 4 epilogue warps: tcgen05.ld of both accumulators, complex
 //               combine, segment sums, IQ store and power.
@@ -101,10 +105,11 @@ struct Args {
   float2* partial;  // kMaxCtas x kPartialPerCta segment sums
   int ns, nc, na, nt, nv;
   double c, fs, fd, fn;
-  int frames;      // frames per pass (multiple of 8, <= 128)
+  int frames;      // frames of every pass but the last (multiple of 8, <= 128)
+  int last_frames; // frames of the last pass (multiple of 8, <= frames)
   int chunks;      // passes per tile
   int ncols;       // 2 * frames
-  int nbox;        // TMA boxes per plane
+  int nbox;        // TMA boxes per plane of a full pass (the stage layout)
   int ntiles;
   int* err;
 };
@@ -218,6 +223,81 @@ __device__ __forceinline__ void put_row(unsigned char* a_hi, unsigned char* a_lo
   }
 }
 
+// Two coefficients rounded to a packed 16-bit pair (c0 in the low half) and the
+// pair of their rounding residuals, rounded again: the hi / lo split of both
+// taps of one A row in two conversions.
+template <bool BF16>
+__device__ __forceinline__ void split_pair(float c0, float c1, uint32_t& hi, uint32_t& lo) {
+  if constexpr (BF16) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(c0, c1);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(c0 - __low2float(h), c1 - __high2float(h));
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+  } else {
+    const __half2 h = __floats2half2_rn(c0, c1);
+    const __half2 l = __floats2half2_rn(c0 - __low2float(h), c1 - __high2float(h));
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+  }
+}
+
+// The eight 32-bit words of a 16-column row whose only nonzero entries are the
+// packed pair v at columns r, r + 1 (r = -1: an all-zero row).
+struct RowPlace {
+  int word;   // word holding column r (-2 when the row is empty)
+  int shift;  // 0 or 16: bit offset of column r in that word
+  __device__ __forceinline__ explicit RowPlace(int r) : word(r >= 0 ? r >> 1 : -2), shift((r & 1) << 4) {}
+  __device__ __forceinline__ uint32_t at(int i, uint32_t v) const {
+    const uint32_t first = v << shift;                      // column r (and r + 1 when r is even)
+    const uint32_t second = __funnelshift_l(v, 0u, shift);  // column r + 1 when r is odd
+    return i == word ? first : (i == word + 1 ? second : 0u);
+  }
+};
+
+// Writes the real (row m, m even) and imaginary (row m + 1) A rows of one voxel
+// into a K-major no-swizzle 128 x 16 matrix: four 16-byte stores, (row, K core)
+// pieces at offsets +0 / +16 / +128 / +144.  Lanes whose 8-row group is odd
+// swap the row order of each store pair, so that every store instruction of
+// the warp spreads over all 32 banks (four wavefronts for 512 bytes).
+__device__ __forceinline__ void put_rows(unsigned char* a, int m, const RowPlace& pl, uint32_t re, uint32_t im) {
+  const bool odd = (m >> 3) & 1;
+  const uint32_t base = uint32_t((m >> 3) * 256 + (m & 7) * 16);
+#pragma unroll
+  for (int kc = 0; kc < 2; ++kc) {
+    uint4 pr, pi;
+    pr.x = pl.at(4 * kc + 0, re);
+    pr.y = pl.at(4 * kc + 1, re);
+    pr.z = pl.at(4 * kc + 2, re);
+    pr.w = pl.at(4 * kc + 3, re);
+    pi.x = pl.at(4 * kc + 0, im);
+    pi.y = pl.at(4 * kc + 1, im);
+    pi.z = pl.at(4 * kc + 2, im);
+    pi.w = pl.at(4 * kc + 3, im);
+    const uint32_t o = base + 128u * kc;
+    *reinterpret_cast<uint4*>(a + o + (odd ? 16u : 0u)) = odd ? pi : pr;
+    *reinterpret_cast<uint4*>(a + o + (odd ? 0u : 16u)) = odd ? pr : pi;
+  }
+}
+
+// mbarrier.expect_tx without an arrival: the writing warp's 32 lanes arrive
+// later, once the coefficient rows are in shared memory.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// Bounded wait with the already-complete case inline (no call on the fast path).
+__device__ __forceinline__ bool wait_phase(uint64_t* bar, uint32_t parity, int* err, int code) {
+  return mbar_test(bar, parity) || mbar_wait(bar, parity, err, code);
+}
+
+// Frames of pass `chunk`: full passes of p.frames, the last one p.last_frames
+// (frames beyond nt are zero-filled by TMA and never stored).
+__device__ __forceinline__ int pass_frames(const Args& p, int chunk) {
+  return chunk == p.chunks - 1 ? p.last_frames : p.frames;
+}
+__device__ __forceinline__ int pass_boxes(int frames) { return (2 * frames + kBoxCols - 1) / kBoxCols; }
+
 // exp(+j 2 pi fd tau) with the cycle count reduced in float64.
 __device__ __forceinline__ float2 demod_phase(double fd, double tau) {
   double cyc = fd * tau;
@@ -298,7 +378,8 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
       }
     }
     bool ok = true;
-    const uint32_t tx_bytes = uint32_t(kPlanes * p.nbox * kBoxBytes);
+    int nbox = p.nbox;  // boxes per plane of the current item's pass
+    uint32_t tx_bytes = uint32_t(kPlanes * nbox * kBoxBytes);
     const float sc = kCoefScale<BF16X3>;
     auto builders_sync = [] { asm volatile("bar.sync 1, %0;" ::"n"(kBuilders * 32) : "memory"); };
     // Claims the next ring stage (uniform in the warp) and waits until it is free.
@@ -307,7 +388,23 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
       if (lane == 0) mine = uint32_t(atomicAdd(counter, 1));
       k = __shfl_sync(0xffffffffu, mine, 0);
       return __all_sync(0xffffffffu,
-                        mbar_wait(&empty[k % STAGES], ((k / STAGES) & 1) ^ 1, p.err, kErrWaitEmpty));
+                        wait_phase(&empty[k % STAGES], ((k / STAGES) & 1) ^ 1, p.err, kErrWaitEmpty));
+    };
+    // Issues the window copies of a claimed stage before its coefficient rows
+    // are written (the copy's latency overlaps the row stores); the warp's 32
+    // arrivals on full[s] follow the rows.
+    auto issue_window = [&](uint32_t s, unsigned char* stage, int config, int col0, int row, int slab) {
+      const CUtensorMap* mh = config ? &map_cr_hi : &map_rc_hi;
+      const CUtensorMap* ml = config ? &map_cr_lo : &map_rc_lo;
+      if (lane == 0) mbar_expect_tx(&full[s], tx_bytes);
+      __syncwarp();
+      unsigned char* b0 = stage + 4 * kAMatBytes;
+      if (lane < kPlanes * nbox) {
+        const bool second = lane >= nbox;
+        const int j = second ? lane - nbox : lane;
+        tma_load_3d(b0 + (second ? p.nbox : 0) * kBoxBytes + j * kBoxBytes, second ? ml : mh, &full[s],
+                    col0 + j * kBoxCols, row, slab);
+      }
     };
     // Stages the window [row, row + 16) x [col0, col0 + ncols) of every plane.
     auto stage_window = [&](uint32_t s, unsigned char* stage, int config, int col0, int row, int slab) {
@@ -316,9 +413,9 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
       if (lane == 0) mbar_arrive_expect_tx(&full[s], tx_bytes);
       __syncwarp();
       unsigned char* b0 = stage + 4 * kAMatBytes;
-      if (lane < kPlanes * p.nbox) {
-        const bool second = lane >= p.nbox;
-        const int j = second ? lane - p.nbox : lane;
+      if (lane < kPlanes * nbox) {
+        const bool second = lane >= nbox;
+        const int j = second ? lane - nbox : lane;
         tma_load_3d(b0 + (second ? p.nbox : 0) * kBoxBytes + j * kBoxBytes, second ? ml : mh, &full[s],
                     col0 + j * kBoxCols, row, slab);
       }
@@ -327,6 +424,8 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
     for (int item = blockIdx.x; item < work_items; item += gridDim.x) {
       const int tile = item / p.chunks, chunk = item % p.chunks;
       const int col0 = 2 * chunk * p.frames;
+      nbox = pass_boxes(pass_frames(p, chunk));
+      tx_bytes = uint32_t(kPlanes * nbox * kBoxBytes);
       // Voxels of this lane: slots lane + 32 j (group = slot / 64).
       double px[4], pz[4], py[4];
       bool pv[4];
@@ -389,14 +488,15 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
             lo = __reduce_min_sync(0xffffffffu, lo);
             hi = __reduce_max_sync(0xffffffffu, hi);
             if (lo == INT_MAX) continue;  // no voxel of the tile sees this slab
-            float2 c0[4], c1[4];
+            // Hi / lo 16-bit pairs of each voxel's real and imaginary A rows.
+            uint32_t re_hi[4], re_lo[4], im_hi[4], im_lo[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
               const float2 pt = tx_phase[(config * p.na + a) * kVox + lane + 32 * j];
               const float2 ph = make_float2(pt.x * ph_rx[j].x - pt.y * ph_rx[j].y, pt.x * ph_rx[j].y + pt.y * ph_rx[j].x);
               // Coefficients of x[i0] and x[i0 + 1]: phase * (1 - w) and phase * w (scaled).
-              c0[j] = make_float2(sc * ph.x * (1.f - w[j]), sc * ph.y * (1.f - w[j]));
-              c1[j] = make_float2(sc * ph.x * w[j], sc * ph.y * w[j]);
+              split_pair<BF16X3>(sc * ph.x * (1.f - w[j]), sc * ph.x * w[j], re_hi[j], re_lo[j]);
+              split_pair<BF16X3>(sc * ph.y * (1.f - w[j]), sc * ph.y * w[j], im_hi[j], im_lo[j]);
             }
             const int slab = ch * p.na + a;
             for (int base = lo; base <= hi; base += kRows - 1) {
@@ -405,20 +505,20 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
               if (!ok) continue;  // failed: keep the control flow, skip the work
               const uint32_t s = k % STAGES;
               unsigned char* stage = stages + size_t(s) * stage_bytes;
+              issue_window(s, stage, config, col0, base, slab);
 #pragma unroll
               for (int j = 0; j < 4; ++j) {
                 const int r = i0[j] - base;
-                const int rr = (i0[j] >= 0 && r >= 0 && r < kRows - 1) ? r : -1;
+                const RowPlace pl((i0[j] >= 0 && r >= 0 && r < kRows - 1) ? r : -1);
                 const int g = j >> 1;                          // slots 0-63 -> group 0, 64-127 -> group 1
                 const int m = 2 * (lane + 32 * (j & 1));       // A row of the voxel within its group
                 unsigned char* a_hi = stage + (2 * g) * kAMatBytes;
-                unsigned char* a_lo = a_hi + kAMatBytes;
-                put_row<BF16X3>(a_hi, a_lo, m, rr, c0[j].x, c1[j].x);
-                put_row<BF16X3>(a_hi, a_lo, m + 1, rr, c0[j].y, c1[j].y);
+                put_rows(a_hi, m, pl, re_hi[j], im_hi[j]);
+                put_rows(a_hi + kAMatBytes, m, pl, re_lo[j], im_lo[j]);
               }
               if (lane == 0) meta[s] = kStep;
               fence_async_smem();
-              stage_window(s, stage, config, col0, base, slab);
+              mbar_arrive(&full[s]);
               ++steps;
             }
           }
@@ -476,7 +576,9 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
   } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------------- MMA --
     if (lane == 0) {
-      const uint32_t idesc = instr_desc(BF16X3, 128, p.ncols);
+      // N of the current item's pass; the item advances at every tile-end marker.
+      int mma_item = blockIdx.x;
+      uint32_t idesc = instr_desc(BF16X3, 128, 2 * pass_frames(p, mma_item % p.chunks));
       uint32_t k = 0, flushes = 0;
       bool need_empty = false;  // a flush is outstanding: the epilogue must drain TMEM first
       bool issued = false;      // MMAs issued since the last flush
@@ -492,7 +594,7 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
       };
       for (;;) {
         const int s = k % STAGES;
-        if (!mbar_wait(&full[s], (k / STAGES) & 1, p.err, kErrWaitFull)) break;
+        if (!wait_phase(&full[s], (k / STAGES) & 1, p.err, kErrWaitFull)) break;
         const int m = meta[s];
         if (m == kFinish) break;
         if (need_empty) {
@@ -504,6 +606,8 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
           flush(issued ? kAccFinal : kAccFinalEmpty);
           mbar_arrive(&empty[s]);
           ++k;
+          mma_item += gridDim.x;
+          if (mma_item < work_items) idesc = instr_desc(BF16X3, 128, 2 * pass_frames(p, mma_item % p.chunks));
           continue;
         }
         const uint32_t st = smem_u32(stages + size_t(s) * stage_bytes);
@@ -541,6 +645,7 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
     for (int item = blockIdx.x; item < work_items && !fail; item += gridDim.x) {
       const int tile = item / p.chunks, chunk = item % p.chunks;
       const int f0 = chunk * p.frames;
+      const int frames = pass_frames(p, chunk);
       for (int nflush = 0;; ++nflush) {
         if (!__all_sync(0xffffffffu, mbar_wait(acc_full, flushes & 1, p.err, kErrWaitFull))) {
           fail = true;
@@ -556,7 +661,7 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
           const size_t qv = size_t(tile) * kVox + kGroupVox * g + vg;
           const unsigned v = qv < size_t(p.nv) ? (p.order ? p.order[qv] : unsigned(qv)) : UINT_MAX;
           float power = 0.f;
-          for (int c0 = 0; c0 < p.ncols; c0 += 32) {
+          for (int c0 = 0; c0 < 2 * frames; c0 += 32) {
             float val[32];
             if (kind != kAccFinalEmpty) {
               tmem_ld32(tmem + (uint32_t(32 * q) << 16) + 256u * g + uint32_t(c0), val);
@@ -569,7 +674,7 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
               const int fl = (c0 >> 1) + i;
-              prev[i] = (nflush > 0 && is_p && fl < p.frames) ? pcol[size_t(fl) * kGroupVox] : make_float2(0.f, 0.f);
+              prev[i] = (nflush > 0 && is_p && fl < frames) ? pcol[size_t(fl) * kGroupVox] : make_float2(0.f, 0.f);
             }
             // The partner lane holds the other half (P <-> Q) of the same voxel.
 #pragma unroll
@@ -577,7 +682,7 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
               const float other_re = __shfl_xor_sync(0xffffffffu, val[2 * i], 1);
               const float other_im = __shfl_xor_sync(0xffffffffu, val[2 * i + 1], 1);
               const int fl = (c0 >> 1) + i;  // frame within the pass
-              if (is_p && fl < p.frames) {
+              if (is_p && fl < frames) {
                 // P lane: D = (P_re - Q_im, P_im + Q_re).
                 float2 acc = make_float2((val[2 * i] - other_im) * (1.0f / kCoefScale<BF16X3>) + prev[i].x,
                                          (val[2 * i + 1] + other_re) * (1.0f / kCoefScale<BF16X3>) + prev[i].y);

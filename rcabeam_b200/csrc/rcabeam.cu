@@ -272,9 +272,15 @@ static bool tc_eligible(const void* const* planes, int count, size_t nt) {
 
 // Shared memory of the tensor-core OPW for nt frames and na angles (0 if it cannot run).
 // Shared memory of the tensor-core kernel with `stages` ring stages (0: does not fit).
+// Frame passes of the tensor-core OPW: full passes of 128 frames (N = 256, four
+// whole 64-column boxes per plane) and a last pass with the remainder rounded up
+// to 8 frames, which stages fewer boxes than equal passes would.
+static size_t tc_full_frames(size_t nt) {
+  return nt > size_t(tc::kMaxFrames) ? size_t(tc::kMaxFrames) : (nt + 7) / 8 * 8;
+}
+
 static size_t tc_smem_bytes(bool bf16x3, size_t nt, size_t na, int stages = tc::kStages) {
-  const size_t chunks = (nt + tc::kMaxFrames - 1) / tc::kMaxFrames;
-  const size_t frames = ((nt + chunks - 1) / chunks + 7) / 8 * 8;
+  const size_t frames = tc_full_frames(nt);
   const int nbox = int((2 * frames + tc::kBoxCols - 1) / tc::kBoxCols);
   size_t smem = (bf16x3 ? tc::Layout<true>::bytes(nbox, int(na), stages)
                         : tc::Layout<false>::bytes(nbox, int(na), stages)) + 1024;
@@ -311,9 +317,9 @@ static rcabeam_status run_tc(tc::Args a) {
     if ((smem = tc_smem_bytes(BF16X3, nt, size_t(a.na), stages))) break;
   if (!smem) return RCABEAM_ERROR_ARGUMENT;
   a.chunks = int((nt + tc::kMaxFrames - 1) / tc::kMaxFrames);
-  int frames = int((nt + a.chunks - 1) / a.chunks);
-  frames = (frames + 7) / 8 * 8;
+  const int frames = int(tc_full_frames(nt));
   a.frames = frames;
+  a.last_frames = int((nt - size_t(frames) * size_t(a.chunks - 1) + 7) / 8 * 8);
   a.ncols = 2 * frames;
   a.nbox = (a.ncols + tc::kBoxCols - 1) / tc::kBoxCols;
   a.ntiles = int((size_t(a.nv) + tc::kVox - 1) / tc::kVox);
@@ -364,8 +370,6 @@ static rcabeam_status ensemble_impl(const void* rc, const void* cr, const float*
   if (ns > INT32_MAX || nc > INT32_MAX || na > INT32_MAX || nt > INT32_MAX || nv > INT32_MAX ||
       nc * na > INT32_MAX || na > 4096)
     return RCABEAM_ERROR_ARGUMENT;
-  // St-SW is outside this build's scope.
-  if (method == 4) return RCABEAM_ERROR_ARGUMENT;
   if (cudaMemsetAsync(pd, 0, 2 * nv * sizeof(float), 0) != cudaSuccess) return RCABEAM_ERROR_CUDA;
   das::Args a{};
   a.rc = rc;
@@ -391,6 +395,25 @@ static rcabeam_status ensemble_impl(const void* rc, const void* cr, const float*
     dim3 grid(unsigned((nv + generic::kWarps - 1) / generic::kWarps),
               unsigned((nt + 32 * generic::kRegFrames - 1) / (32 * generic::kRegFrames)));
     generic::ensemble_nonlinear<2><<<grid, generic::kWarps * 32>>>(a);
+    return launch_status();
+  }
+  if (method == 4) {
+    // St-SW: series into the caller's workspace (nv k^2 nt complex64), then
+    // energies, pair sums, raw weights and the XDoppler magnitude.
+    constexpr int kStswFrames = 4;
+    const unsigned blocks = unsigned((nv + generic::kWarps - 1) / generic::kWarps);
+    dim3 grid(blocks, unsigned((nt + 32 * kStswFrames - 1) / (32 * kStswFrames)));
+    float2* series = static_cast<float2*>(workspace);
+    if (k == 2) {
+      generic::stsw_series<2, kStswFrames><<<grid, generic::kWarps * 32>>>(a, series);
+      generic::stsw_finish<2><<<blocks, generic::kWarps * 32>>>(pd, weights, series, nv, int(nt));
+    } else if (k == 3) {
+      generic::stsw_series<3, kStswFrames><<<grid, generic::kWarps * 32>>>(a, series);
+      generic::stsw_finish<3><<<blocks, generic::kWarps * 32>>>(pd, weights, series, nv, int(nt));
+    } else {
+      generic::stsw_series<4, kStswFrames><<<grid, generic::kWarps * 32>>>(a, series);
+      generic::stsw_finish<4><<<blocks, generic::kWarps * 32>>>(pd, weights, series, nv, int(nt));
+    }
     return launch_status();
   }
   // The caller owns 2 * nv * (nc + na) float4 of scratch (reference rcabeam.h:196).

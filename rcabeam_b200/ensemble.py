@@ -67,8 +67,8 @@ def _run(rc, cr, angles, t_start, grid, geom: RCAGeometry, method, k: int, retur
         raise ValueError("Sound speed and sampling frequency must be finite and positive")
     if geom.fnumber is not None and (not np.isfinite(geom.fnumber) or geom.fnumber <= 0):
         raise ValueError("F-number must be positive or None")
-    if method == "st_sw":
-        raise ValueError("St-SW is not provided by this implementation")
+    if method == "st_sw" and (k < 2 or k > 4 or len(angles) < k):
+        raise ValueError("St-SW requires 2 <= k <= 4 and at least k angles")
     starts = np.ascontiguousarray(np.broadcast_to(np.asarray(t_start, dtype=np.float32), (len(angles),)))
     if not all(np.isfinite(a).all() for a in (angles, starts, geom.x_el, geom.y_el)):
         raise ValueError("Geometry and sample starts must be finite")
@@ -78,6 +78,7 @@ def _run(rc, cr, angles, t_start, grid, geom: RCAGeometry, method, k: int, retur
     pd = np.empty((nv, 2), dtype=np.float32)
     planes = 2 if method == "apertures" else 1
     signal = np.empty((nv * planes if return_signal else 0, nt), dtype=np.complex64)
+    weights = np.empty(nv if method == "st_sw" else 0, dtype=np.float32)
     raw_upload_seconds = _cuda_impl.ensemble_from_channels(
         np.ascontiguousarray(rc, dtype=np.complex64),
         np.ascontiguousarray(cr, dtype=np.complex64),
@@ -88,7 +89,7 @@ def _run(rc, cr, angles, t_start, grid, geom: RCAGeometry, method, k: int, retur
         starts,
         pd,
         signal,
-        None,
+        weights,
         float(geom.c),
         float(geom.fs),
         float(geom.f_demod),
@@ -99,6 +100,10 @@ def _run(rc, cr, angles, t_start, grid, geom: RCAGeometry, method, k: int, retur
     )
     if timings is not None:
         timings["raw_upload_seconds"] = raw_upload_seconds
+    if method == "st_sw":
+        # Raw weights normalized by the full-volume peak (reference ensemble.py:127-129).
+        peak = weights.max()
+        pd[:, 0] *= weights / peak if peak > 0 else 0
     if return_signal:
         signal_shape = (*shape, 2, nt) if method == "apertures" else (*shape, nt)
         return pd[:, 0].reshape(shape), signal.reshape(signal_shape)

@@ -7,7 +7,15 @@ clutter-filtered power Doppler.  All buffers are allocated once; ``run``
 launches every stage on the default stream without host synchronization
 except the final solver-status check, and records CUDA events per stage.
 ``run_host`` adds the pinned host -> device upload of the channels and the
-device -> host read of the power, the boundary a host caller sees.  With a
+device -> host read of the power, the boundary a host caller sees.
+
+``domain="channel"`` is the reference's channel-domain variant
+(clutter_pipeline.py:85-91, 121-123): one temporal basis estimated over the
+channel Casorati rows of both apertures ((samples x channels x angles) x
+frames each), both apertures filtered before packing, then OPW and the mean
+|IQ|^2 from the DAS kernel's power output (no IQ ensemble is stored).  DAS is
+linear and acts on every frame alike, so for a given basis both domains give
+the same filtered IQ; they differ in the rows the basis is estimated from.  With a
 process group, each rank reconstructs its x slab of the grid
 (``sharded.shard_grid``) and the clutter basis is estimated over every rank's
 rows (one MAX and one SUM all-reduce, ``rcabeam_b200.sharded``).
@@ -23,6 +31,7 @@ from rcabeam_b200.gpu_clutter import Gram
 from rcabeam_b200.sim import RCAGeometry, scan_coords
 
 _STAGES = ("pack", "das", "gram", "eig", "power")
+_CHANNEL_STAGES = ("gram", "eig", "filter", "pack", "das")
 
 
 class FilteredOpw:
@@ -30,7 +39,7 @@ class FilteredOpw:
 
     def __init__(self, channel_shape, angles, t_start, grid, geom: RCAGeometry, *, rank_start: int = 3,
                  rank_stop: int | None = None, precision: str = "complex128", iq_storage: str = "float32",
-                 group=None):
+                 group=None, domain: str = "beamformed"):
         ns, nc, na, nt = (int(n) for n in channel_shape)
         self.shape = (len(grid[0]), len(grid[1]), len(grid[2]))
         self.channel_shape = (ns, nc, na, nt)
@@ -40,6 +49,11 @@ class FilteredOpw:
         self.rank = (int(rank_start), stop)
         self.precision = precision
         self.group = group  # process group whose ranks hold the other x slabs (rcabeam_b200.sharded)
+        if domain not in ("beamformed", "channel"):
+            raise ValueError("Unknown filter domain")
+        if domain == "channel" and group is not None:
+            raise ValueError("Channel-domain filtering runs on one device")
+        self.domain = domain
         if iq_storage not in ("float32", "float16", "bf16x2"):
             raise ValueError("IQ storage must be float32, float16 or bf16x2")
         if iq_storage == "bf16x2" and nt % 4:
@@ -63,7 +77,10 @@ class FilteredOpw:
         self.range_error = torch.zeros(1, dtype=torch.int32, device=dev)
         self.geometry = torch.empty(_cuda_impl.workspace_bytes(self.nv, nc, na), dtype=torch.uint8, device=dev)
         self.pd = torch.empty((self.nv, 2), dtype=torch.float32, device=dev)
-        self.iq = torch.empty((self.nv, nt), dtype=torch.complex64, device=dev)
+        # Beamformed domain: the IQ ensemble (Casorati rows); channel domain: the filtered channels.
+        self.iq = torch.empty((self.nv, nt), dtype=torch.complex64, device=dev) if domain == "beamformed" else None
+        self.filtered = ([torch.empty(self.channel_shape, dtype=torch.complex64, device=dev) for _ in range(2)]
+                         if domain == "channel" else None)
         self.gram = Gram(nt, dev)
         self.power = torch.empty(self.nv, dtype=torch.float64, device=dev)
         self.host_power = torch.empty(self.nv, dtype=torch.float64, pin_memory=True)
@@ -87,9 +104,59 @@ class FilteredOpw:
 
     def run(self, rc: torch.Tensor, cr: torch.Tensor) -> torch.Tensor:
         """Filtered power of resident complex64 RC/CR channels ``(ns, nc, na, nt)``."""
+        if self.domain == "channel":
+            return self._run_channel(rc, cr)
+        ev = self.events
+        ev[0].record()
+        self._pack(rc, cr)
+        ev[1].record()
+        self._das(self.iq)
+        ev[2].record()
+        self.gram.accumulate((self.iq,), self.precision, self.group)
+        ev[3].record()
+        self.gram.decompose()
+        ev[4].record()
+        if self.rank[0] == self.rank[1]:
+            self.power.zero_()
+        else:
+            self._select_vectors()
+            _lib.call("rcabeam_project_device", self.iq.data_ptr(), None, self.power.data_ptr(), self.nv,
+                      self.channel_shape[3], 0, self.vectors.data_ptr(), self.k, 1 if self.subtract else 0)
+        ev[5].record()
+        self.last_das_event_ms = (ev[1], ev[2])
+        return self.power.view(self.shape)
+
+    def _run_channel(self, rc: torch.Tensor, cr: torch.Tensor) -> torch.Tensor:
+        """Channel domain: shared basis of the RC and CR channel rows, filter, pack, OPW power."""
         ns, nc, na, nt = self.channel_shape
         ev = self.events
         ev[0].record()
+        self.gram.accumulate((rc, cr), self.precision)
+        ev[1].record()
+        self.gram.decompose()
+        ev[2].record()
+        rows = ns * nc * na
+        if self.rank[0] != self.rank[1]:
+            self._select_vectors()
+            for src, dst in zip((rc, cr), self.filtered):
+                _lib.call("rcabeam_project_device", src.data_ptr(), dst.data_ptr(), None, rows, nt, 0,
+                          self.vectors.data_ptr(), self.k, (1 if self.subtract else 0) | 2)
+        ev[3].record()
+        if self.rank[0] == self.rank[1]:
+            self.power.zero_()
+            for e in ev[4:]:
+                e.record()
+        else:
+            self._pack(*self.filtered)
+            ev[4].record()
+            self._das(None)
+            self.power.copy_(self.pd[:, 0])
+            ev[5].record()
+        self.last_das_event_ms = (ev[4], ev[5])
+        return self.power.view(self.shape)
+
+    def _pack(self, rc: torch.Tensor, cr: torch.Tensor) -> None:
+        ns, nc, na, nt = self.channel_shape
         if self.storage == "float16":
             self.range_error.zero_()
             for src, dst in zip((rc, cr), self.packed):
@@ -103,31 +170,21 @@ class FilteredOpw:
         else:
             for src, dst in zip((rc, cr), self.packed):
                 _lib.call("rcabeam_pack_ensemble_device", src.data_ptr(), dst.data_ptr(), ns, nc, na, nt)
-        ev[1].record()
+
+    def _das(self, iq: torch.Tensor | None) -> None:
+        """OPW of the packed channels: power into pd, IQ into ``iq`` when given."""
+        ns, nc, na, nt = self.channel_shape
+        signal = None if iq is None else iq.data_ptr()
         if self.storage == "bf16x2":
             _lib.call("rcabeam_opw_tc_device", self.packed[0].data_ptr(), self.packed_lo[0].data_ptr(),
                       self.packed[1].data_ptr(), self.packed_lo[1].data_ptr(), self.scan.data_ptr(),
                       self.xe.data_ptr(), self.ye.data_ptr(), self.angles.data_ptr(), self.starts.data_ptr(),
-                      self.pd.data_ptr(), self.iq.data_ptr(), self.geometry.data_ptr(), ns, nc, na, nt, self.nv,
+                      self.pd.data_ptr(), signal, self.geometry.data_ptr(), ns, nc, na, nt, self.nv,
                       *self.consts, 1)
         else:
             _cuda_impl.opw_from_packed(self.packed[0], self.packed[1], self.scan, self.xe, self.ye, self.angles,
-                                       self.starts, self.pd, self.iq, self.geometry, ns, nc, na, nt, *self.consts,
+                                       self.starts, self.pd, iq, self.geometry, ns, nc, na, nt, *self.consts,
                                        self.half, synchronize=False)
-        ev[2].record()
-        self.gram.accumulate((self.iq,), self.precision, self.group)
-        ev[3].record()
-        self.gram.decompose()
-        ev[4].record()
-        if self.rank[0] == self.rank[1]:
-            self.power.zero_()
-        else:
-            self._select_vectors()
-            _lib.call("rcabeam_project_device", self.iq.data_ptr(), None, self.power.data_ptr(), self.nv, nt, 0,
-                      self.vectors.data_ptr(), self.k, 1 if self.subtract else 0)
-        ev[5].record()
-        self.last_das_event_ms = (ev[1], ev[2])
-        return self.power.view(self.shape)
 
     def check(self) -> None:
         """Synchronize and raise on solver or staging-pipeline failures."""
@@ -153,13 +210,17 @@ class FilteredOpw:
 
     def stage_ms(self) -> dict:
         torch.cuda.synchronize()
-        return {name: round(self.events[i].elapsed_time(self.events[i + 1]), 3) for i, name in enumerate(_STAGES)}
+        names = _CHANNEL_STAGES if self.domain == "channel" else _STAGES
+        return {name: round(self.events[i].elapsed_time(self.events[i + 1]), 3) for i, name in enumerate(names)}
 
     def launches_per_step(self) -> int:
         """Kernels of this library launched per ``run``: pack x2, voxel order (bounding box,
         Morton codes, 4 radix-sort passes), DAS (one persistent tensor-core launch, or main +
-        tail staged launches), scale, Gram, Gram finish, projection."""
+        tail staged launches), scale, Gram, Gram finish, projection (channel domain: per
+        aperture scale, Gram and projection)."""
         das = 1 if self.storage != "float32" and self.channel_shape[3] % 4 == 0 else 2
+        if self.domain == "channel":  # scale x2, Gram x2, finish, projection x2, pack x2, order, DAS
+            return 5 + 2 + 2 + 6 + das
         return 2 + 6 + das + 4
 
 

@@ -41,7 +41,7 @@ def _quant(z):
 
 
 @pytest.mark.parametrize("storage", ["float16", "bf16x2"])
-@pytest.mark.parametrize("frames", [4, 8, 200, 300])
+@pytest.mark.parametrize("frames", [4, 8, 136, 200, 256, 300])
 @pytest.mark.parametrize("fnumber", [None, 1.0])
 def test_tc_small_random(storage, frames, fnumber):
     grid = (np.array([0.0, 0.008]), np.array([0.001, 0.007, 0.03]), np.array([0.0]))

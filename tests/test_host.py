@@ -88,6 +88,35 @@ def test_python_validation_messages():
     with pytest.raises(ValueError, match="F-number"):
         rb.ensemble_pd_from_channels(data, data, np.zeros(2), 1e-6, (np.zeros(1), np.ones(1), np.zeros(1)),
                                      RCAGeometry(np.zeros(1), np.zeros(1), fnumber=-1.0))
+    # St-SW subsets: 2 <= k <= 4 and at least k angles (reference ensemble.py:80-81).
+    for k, angles in ((1, 2), (5, 2), (3, 2)):
+        with pytest.raises(ValueError, match="St-SW requires"):
+            rb.ensemble_pd_from_channels(data[:, :, :angles], data[:, :, :angles], np.zeros(angles), 1e-6,
+                                         (np.zeros(1), np.ones(1), np.zeros(1)), g1, method="st_sw", k=k)
+
+
+def test_st_sw_argument_rejection_without_gpu(built_library):
+    """Method 4 needs weights and workspace, no signal, 2 <= k <= 4 and na >= k (reference ensemble.cu:671-673)."""
+    lib = _lib.lib()
+    b = ctypes.c_void_p(16)
+    head = [b] * 8  # rc, cr, scan, xe, ye, angles, starts, pd
+    ok_tail = (4, 1, 2, 3, 1, 1540.0, 1.0, 0.0, -1.0, 4)
+    assert lib.rcabeam_ensemble_device(*head, None, None, b, b, *ok_tail, 2) == 2   # no weights
+    assert lib.rcabeam_ensemble_device(*head, None, b, None, b, *ok_tail, 2) == 2   # no workspace
+    assert lib.rcabeam_ensemble_device(*head, b, b, b, b, *ok_tail, 2) == 2        # signal given
+    assert lib.rcabeam_ensemble_device(*head, None, b, b, b, *ok_tail, 1) == 2     # k < 2
+    assert lib.rcabeam_ensemble_device(*head, None, b, b, b, *ok_tail, 3) == 2     # na = 2 < k
+    assert lib.rcabeam_ensemble_device(*head, None, b, b, b, *ok_tail, 5) == 2     # k > 4
+    # The no-allocation entry point has no series workspace and rejects St-SW.
+    assert lib.rcabeam_ensemble_static_device(*head, None, 4, 1, 2, 3, 1, 1540.0, 1.0, 0.0, -1.0, 4) == 2
+
+
+def test_filtered_pipeline_domain_rejected_without_gpu():
+    from rcabeam_b200.pipeline import FilteredOpw
+
+    with pytest.raises(ValueError, match="domain"):
+        FilteredOpw((8, 2, 1, 4), np.zeros(1), 1e-6, (np.zeros(1), np.ones(1), np.zeros(1)),
+                    RCAGeometry(np.zeros(2), np.zeros(2)), domain="image")
 
 
 def test_voxel_order_matches_reference_golden():

@@ -25,7 +25,7 @@ import numpy as np
 import pytest
 import torch
 
-from oracle import das
+from oracle import das, methods
 from rcabeam_b200 import _cuda_impl, _lib
 from rcabeam_b200.sim import RCAGeometry, scan_coords
 from tests._cases import oracle_inputs, random_case, rel_l2
@@ -128,6 +128,28 @@ class Case:
         return pd[:, 0].cpu().numpy(), None if sig is None else sig.cpu().numpy()
 
 
+    def stsw(self, handle, k, tile=4096):
+        """St-SW (method 4) XDoppler power and raw weights of one library, in voxel
+        tiles with a k^2 nt series workspace per tile (reference python.cpp:553-565)."""
+        (prc, pcr), _ = self.packed(handle)
+        nv, nt = self.nv, self.nt
+        tile = min(tile, nv)
+        pd = torch.zeros((nv, 2), dtype=torch.float32, device="cuda")
+        weights = torch.zeros(nv, dtype=torch.float32, device="cuda")
+        work = torch.empty(tile * k * k * nt, dtype=torch.complex64, device="cuda")
+        geo = torch.empty(2 * tile * (self.nc + self.na) * 16, dtype=torch.uint8, device="cuda")
+        for start in range(0, nv, tile):
+            count = min(tile, nv - start)
+            st = handle.rcabeam_ensemble_device(_p(prc), _p(pcr), self.scan.data_ptr() + 12 * start, _p(self.xe),
+                                                _p(self.ye), _p(self.angles), _p(self.starts),
+                                                pd.data_ptr() + 8 * start, None, weights.data_ptr() + 4 * start,
+                                                _p(work), _p(geo), self.ns, self.nc, self.na, nt, count,
+                                                *self.consts, 4, k)
+            _ok(st, f"St-SW k={k}")
+        torch.cuda.synchronize()
+        return pd[:, 0].cpu().numpy(), weights.cpu().numpy()
+
+
 def _random(frames, fnumber, seed=5):
     el = (np.arange(16) - 7.5) * 0.2e-3
     # Offsets keep every |v - e| away from an exact f-number aperture tie: at a
@@ -176,6 +198,26 @@ def test_ensemble_methods_match_reference_kernels(ref, method, fnumber, frames):
                         o["fd"], o["fnumber"])
         err_new, err_ref = rel_l2(sig_new, iq), rel_l2(sig_ref, iq)
         assert err_new <= max(err_ref, 1e-5), (err_new, err_ref)
+
+
+@pytest.mark.parametrize("frames", [8, 33])
+@pytest.mark.parametrize("k", [2, 3, 4])
+def test_st_sw_matches_reference_kernels(ref, k, frames):
+    """Method 4: XDoppler power, raw weights and the peak-normalized St-SW power of both
+    libraries; this build is at least as close to the float64 oracle."""
+    case = _random(frames, 1.0)
+    pd_ref, w_ref = case.stsw(ref, k)
+    pd_new, w_new = case.stsw(_lib.lib(), k)
+    assert np.abs(pd_ref).max() > 0 and w_ref.max() > 0
+    assert rel_l2(pd_new, pd_ref) <= TOL
+    assert rel_l2(w_new, w_ref) <= 1e-3
+    power_ref, power_new = pd_ref * w_ref / w_ref.max(), pd_new * w_new / w_new.max()
+    assert rel_l2(power_new, power_ref) <= 1e-3  # the reference's St-SW test tolerance
+    o = case.oracle
+    expected = methods.st_sw_power(case.rc, case.cr, o["scan"], o["xe"], o["ye"], o["angles"], o["starts"], o["c"],
+                                   o["fs"], o["fd"], o["fnumber"], k)
+    err_new, err_ref = rel_l2(power_new, expected), rel_l2(power_ref, expected)
+    assert err_new <= max(err_ref, 1e-4), (err_new, err_ref)
 
 
 @pytest.mark.parametrize("frames", [8, 64])
