@@ -426,6 +426,95 @@ def run_precision(args) -> dict:
             "data": "synthetic seeded scene model", "gpu_launches": None}
 
 
+# ------------------------------------------------------ channel domain --
+def run_channel(args) -> dict:
+    """Channel-domain filtered OPW PD on the full workload (reference clutter_pipeline.py:85-123 with
+    domain="channel"): one basis over the RC + CR channel Casorati rows (2 x 720,896 x 200), both
+    apertures filtered, packed and beamformed to power (no IQ ensemble stored)."""
+    import torch
+
+    from rcabeam_b200 import _lib, pipeline
+    from rcabeam_b200.sim import RCAGeometry
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    el, angles, grid = workload()
+    geom = RCAGeometry(el, el, c=C, fs=FS, f_demod=FD, fnumber=None)
+    gen = torch.Generator(device=dev).manual_seed(1234)
+    rc, cr = pipeline.synthetic_channels((NS, NC, NA, NT), generator=gen, device=dev)
+    units = units_per_step()
+    results, powers = {}, {}
+    for name in ("chosen", "plain"):
+        storage, precision = FORMS[name]
+        plan = pipeline.FilteredOpw((NS, NC, NA, NT), angles, T_START, grid, geom, rank_start=RANK_START,
+                                    precision=precision, iq_storage=storage, domain="channel")
+        steps = args.steps if name == "chosen" else max(1, min(args.steps, 2))
+        elapsed, das_s, stages = _time_form(plan, rc, cr, steps, args.warmup if name == "chosen" else 1, 1)
+        powers[name] = plan.power.clone()
+        results[name] = {"ms_per_ensemble": round(elapsed / steps * 1e3, 3), "steps": steps,
+                         "gsamples_per_s": round(units * steps / elapsed / 1e9, 3), "das_ms": round(das_s * 1e3, 3),
+                         "stages_ms": stages, "iq_storage": storage, "gram_precision": precision,
+                         "gpu_launches_per_step": plan.launches_per_step()}
+        del plan
+        torch.cuda.empty_cache()
+    assert _lib.device_error() == 0
+    ref = powers["plain"]
+    return {"form": "channel", "metric": "channel-domain filtered PD ms/ensemble", "unit": "ms",
+            "higher_is_better": False, "value": results["chosen"]["ms_per_ensemble"], "forms": results,
+            "accuracy": {"chosen_vs_plain_filtered_pd_rel_l2": float(torch.linalg.vector_norm(powers["chosen"] - ref)
+                                                                     / torch.linalg.vector_norm(ref))},
+            "config": {**CONFIG, "domain": "channel"}, "data": "synthetic seeded channel IQ (complex Gaussian)"}
+
+
+# ------------------------------------------------------------- St-SW --
+def run_stsw(args) -> dict:
+    """St-SW (method 4, k = 2, 3, 4) through the C ABI on resident channels of the full shape
+    (512 x 128 x 11 x 200) over a central block of the full grid (default 32 x 64 x 32)."""
+    import torch
+
+    from rcabeam_b200 import _cuda_impl, _lib, pipeline
+    from rcabeam_b200.sim import scan_coords
+
+    global SUBGRID
+    SUBGRID = tuple(args.subgrid) if args.subgrid else (32, 64, 32)
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    el, angles, grid = workload()
+    gen = torch.Generator(device=dev).manual_seed(1234)
+    rc, cr = pipeline.synthetic_channels((NS, NC, NA, NT), generator=gen, device=dev)
+    scan = scan_coords(grid)
+    nv = len(scan)
+    f32 = lambda v: torch.from_numpy(np.ascontiguousarray(v, dtype=np.float32)).to(dev)  # noqa: E731
+    d_scan, d_el, d_ang = f32(scan), f32(el), f32(angles)
+    d_starts = f32(np.full(NA, T_START))
+    pd = torch.empty((nv, 2), dtype=torch.float32, device=dev)
+    weights = torch.empty(nv, dtype=torch.float32, device=dev)
+    units = nv * 2 * NC * NA * NT
+    out = {}
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for k in (2, 3, 4):
+        def step():
+            _cuda_impl.ensemble_from_channels(rc, cr, d_scan, d_el, d_el, d_ang, d_starts, pd, None, weights, C, FS,
+                                              FD, -1.0, 4, k, False)
+        for _ in range(max(1, args.warmup)):
+            step()
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(max(1, args.steps)):
+            step()
+        stop.record()
+        torch.cuda.synchronize()
+        ms = start.elapsed_time(stop) / max(1, args.steps)
+        out[f"k{k}"] = {"ms": round(ms, 2), "gsamples_per_s": round(units / ms / 1e6, 1)}
+    assert _lib.device_error() == 0
+    return {"form": "stsw", "metric": "St-SW Gsamples/s (vox*ch*ang*frm)", "unit": "Gsamples/s",
+            "value": out["k2"]["gsamples_per_s"], "forms": out,
+            "config": {"workload": f"St-SW on a {list(SUBGRID)} block of the full grid, channels "
+                                   f"{NS}x{NC}x{NA}x{NT} c64 per aperture, full aperture", "voxels": nv,
+                       "note": "timed region: pack both apertures + series kernel + finish per voxel tile"},
+            "data": "synthetic seeded channel IQ (complex Gaussian)"}
+
+
 # ------------------------------------------------ differentiation form --
 def run_differentiation(args) -> dict:
     """Grid 64 x 128 x 64, channels (384, 128, 7, 32): forward PD of the whole grid and the
@@ -605,7 +694,8 @@ def main() -> None:
     ap.add_argument("--channels", type=int, default=None, help="reduced channel count for profiling runs")
     ap.add_argument("--subgrid", type=int, nargs=3, default=None, metavar=("NX", "NZ", "NY"),
                     help="central block of the full grid at full resolution (profiling runs)")
-    ap.add_argument("--form", default="filtered", choices=["filtered", "batching", "precision", "differentiation"],
+    ap.add_argument("--form", default="filtered",
+                    choices=["filtered", "batching", "precision", "differentiation", "channel", "stsw"],
                     help="filtered: the filtered-OPW headline; batching, precision, differentiation: the forms")
     ap.add_argument("--rows", type=int, default=128 * 256 * 128, help="Casorati rows of the precision form")
     ap.add_argument("--casorati-frames", type=int, default=400, help="Casorati frames of the precision form")
@@ -616,7 +706,8 @@ def main() -> None:
     args = ap.parse_args()
     if args.form != "filtered":
         if args.impl == "b200" and int(os.environ.get("RANK", "0")) == 0:
-            run = {"batching": run_batching, "precision": run_precision, "differentiation": run_differentiation}
+            run = {"batching": run_batching, "precision": run_precision, "differentiation": run_differentiation,
+                   "channel": run_channel, "stsw": run_stsw}
             print(json.dumps(run[args.form](args)), flush=True)
         return
     global GRID_SHAPE, NT, NC, SUBGRID
