@@ -298,6 +298,19 @@ __device__ __forceinline__ int pass_frames(const Args& p, int chunk) {
 }
 __device__ __forceinline__ int pass_boxes(int frames) { return (2 * frames + kBoxCols - 1) / kBoxCols; }
 
+// Pass of work item `item` (CTA b takes items b, b + G, b + 2G, ...; G = gridDim.x).
+// The passes of a tile are consecutive items, so with G a multiple of the pass
+// count a CTA would always get the same pass -- and the long and short passes
+// would split the CTAs into fast and slow halves that drift apart (losing the
+// lockstep that keeps the windows L2-resident) and finish unevenly.  Rotating
+// the pass by the item's round makes every CTA cycle through all passes; the
+// rotation is a bijection within each tile exactly when G % chunks == 0.
+__device__ __forceinline__ int item_pass(const Args& p, int item) {
+  const int chunk = item % p.chunks;
+  if (gridDim.x % unsigned(p.chunks) != 0) return chunk;
+  return (chunk + item / int(gridDim.x)) % p.chunks;
+}
+
 // exp(+j 2 pi fd tau) with the cycle count reduced in float64.
 __device__ __forceinline__ float2 demod_phase(double fd, double tau) {
   double cyc = fd * tau;
@@ -422,7 +435,7 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
       if (lane != 0) mbar_arrive(&full[s]);
     };
     for (int item = blockIdx.x; item < work_items; item += gridDim.x) {
-      const int tile = item / p.chunks, chunk = item % p.chunks;
+      const int tile = item / p.chunks, chunk = item_pass(p, item);
       const int col0 = 2 * chunk * p.frames;
       nbox = pass_boxes(pass_frames(p, chunk));
       tx_bytes = uint32_t(kPlanes * nbox * kBoxBytes);
@@ -578,7 +591,7 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
     if (lane == 0) {
       // N of the current item's pass; the item advances at every tile-end marker.
       int mma_item = blockIdx.x;
-      uint32_t idesc = instr_desc(BF16X3, 128, 2 * pass_frames(p, mma_item % p.chunks));
+      uint32_t idesc = instr_desc(BF16X3, 128, 2 * pass_frames(p, item_pass(p, mma_item)));
       uint32_t k = 0, flushes = 0;
       bool need_empty = false;  // a flush is outstanding: the epilogue must drain TMEM first
       bool issued = false;      // MMAs issued since the last flush
@@ -607,7 +620,7 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
           mbar_arrive(&empty[s]);
           ++k;
           mma_item += gridDim.x;
-          if (mma_item < work_items) idesc = instr_desc(BF16X3, 128, 2 * pass_frames(p, mma_item % p.chunks));
+          if (mma_item < work_items) idesc = instr_desc(BF16X3, 128, 2 * pass_frames(p, item_pass(p, mma_item)));
           continue;
         }
         const uint32_t st = smem_u32(stages + size_t(s) * stage_bytes);
@@ -643,7 +656,7 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
     uint32_t flushes = 0;
     bool fail = false;
     for (int item = blockIdx.x; item < work_items && !fail; item += gridDim.x) {
-      const int tile = item / p.chunks, chunk = item % p.chunks;
+      const int tile = item / p.chunks, chunk = item_pass(p, item);
       const int f0 = chunk * p.frames;
       const int frames = pass_frames(p, chunk);
       for (int nflush = 0;; ++nflush) {
