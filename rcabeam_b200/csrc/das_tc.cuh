@@ -103,6 +103,7 @@ struct Args {
   float* pd;
   float2* signal;
   float2* partial;  // kMaxCtas x kPartialPerCta segment sums
+  unsigned long long* slot_clock;  // channel slots staged by all CTAs (phase of the herd; never reset)
   int ns, nc, na, nt, nv;
   double c, fs, fd, fn;
   int frames;      // frames of every pass but the last (multiple of 8, <= 128)
@@ -346,6 +347,7 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
   int* counter = reinterpret_cast<int*>(tmem_slot + 1);  // next ring stage to claim
   int* item_steps = counter + 1;                         // steps staged for the current item
   volatile int* acc_kind = item_steps + 1;               // AccKind of the pending flush
+  int* walk_start = item_steps + 2;                      // first channel slot of the current item
   double* angle_tab = reinterpret_cast<double*>(ctrl + 1024);
   double* tx_delay = angle_tab + 3 * p.na;                                   // [2][na][128]
   float2* tx_phase = reinterpret_cast<float2*>(tx_delay + 2 * p.na * kVox);  // [2][na][128]
@@ -466,11 +468,22 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
         tx_delay[e] = ttx;
         tx_phase[e] = demod_phase(p.fd, ttx);
       }
+      // Channel slots u = aperture * nc + channel are walked from the slot the
+      // other CTAs are at (the global slot count over the grid size): static
+      // item assignment lets CTAs drift apart over a long launch, and CTAs in
+      // different slabs together touch more sample windows than L2 holds.
+      // The walk order only changes the order of the float32 sums.
+      if (warp == 0 && lane == 0)
+        *walk_start = int((*reinterpret_cast<volatile unsigned long long*>(p.slot_clock) / gridDim.x) %
+                          (2ull * unsigned(p.nc)));
       builders_sync();
       int steps = 0;
-      for (int config = 0; config < 2; ++config) {
+      const int slots = 2 * p.nc, u0 = *walk_start;
+      for (int i = warp; i < slots; i += kBuilders) {
+        const int u = (u0 + i) % slots;
+        const int config = u / p.nc, ch = u - config * p.nc;
         const float* el = config ? p.ye : p.xe;
-        for (int ch = warp; ch < p.nc; ch += kBuilders) {
+        {  // this channel's receive delays, then its angles' steps
           double trx[4];
           float2 ph_rx[4];
           bool act[4];
@@ -536,6 +549,7 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
             }
           }
         }
+        if (lane == 0) atomicAdd(p.slot_clock, 1ull);
       }
       // Every builder's steps of this item are staged before its markers.
       builders_sync();
@@ -674,20 +688,25 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
           const size_t qv = size_t(tile) * kVox + kGroupVox * g + vg;
           const unsigned v = qv < size_t(p.nv) ? (p.order ? p.order[qv] : unsigned(qv)) : UINT_MAX;
           float power = 0.f;
+          // Earlier segments' sums of 16 frames, loaded one chunk ahead so that
+          // their L2 latency overlaps the previous chunk's TMEM read and combine.
+          float2 prev[16], next[16];
+          auto load_prev = [&](float2 (&dst)[16], int c0) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const int fl = (c0 >> 1) + i;
+              dst[i] = (nflush > 0 && is_p && fl < frames) ? pcol[size_t(fl) * kGroupVox] : make_float2(0.f, 0.f);
+            }
+          };
+          load_prev(prev, 0);
           for (int c0 = 0; c0 < 2 * frames; c0 += 32) {
             float val[32];
+            if (c0 + 32 < 2 * frames) load_prev(next, c0 + 32);
             if (kind != kAccFinalEmpty) {
               tmem_ld32(tmem + (uint32_t(32 * q) << 16) + 256u * g + uint32_t(c0), val);
             } else {
 #pragma unroll
               for (int i = 0; i < 32; ++i) val[i] = 0.f;
-            }
-            // Earlier segments' sums of these 16 frames (loads issued together).
-            float2 prev[16];
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-              const int fl = (c0 >> 1) + i;
-              prev[i] = (nflush > 0 && is_p && fl < frames) ? pcol[size_t(fl) * kGroupVox] : make_float2(0.f, 0.f);
             }
             // The partner lane holds the other half (P <-> Q) of the same voxel.
 #pragma unroll
@@ -707,6 +726,8 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
                 }
               }
             }
+#pragma unroll
+            for (int i = 0; i < 16; ++i) prev[i] = next[i];
           }
           if (last && is_p && v != UINT_MAX) atomicAdd(p.pd + 2 * size_t(v), power / float(p.nt));
         }

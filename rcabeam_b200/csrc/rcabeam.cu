@@ -293,6 +293,24 @@ static size_t tc_smem_bytes(bool bf16x3, size_t nt, size_t na, int stages = tc::
 // are serialized on the default stream, so one buffer per device suffices).
 static __device__ float2 g_tc_partials[tc::kMaxCtas * tc::kPartialPerCta];
 
+// Global channel-slot count of the tensor-core DAS (its phase aligns the CTAs'
+// slab walks; any starting value works, so it is never reset).
+static __device__ unsigned long long g_tc_slot_clock;
+
+static unsigned long long* tc_slot_clock_address() {
+  static std::mutex lock;
+  static unsigned long long* addresses[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> guard(lock);
+  if (!addresses[dev]) {
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_tc_slot_clock) != cudaSuccess) return nullptr;
+    addresses[dev] = static_cast<unsigned long long*>(ptr);
+  }
+  return addresses[dev];
+}
+
 static float2* tc_partials_address() {
   static std::mutex lock;
   static float2* addresses[64] = {};
@@ -344,7 +362,8 @@ static rcabeam_status run_tc(tc::Args a) {
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
     return RCABEAM_ERROR_CUDA;
   a.partial = tc_partials_address();
-  if (!a.partial) return RCABEAM_ERROR_CUDA;
+  a.slot_clock = tc_slot_clock_address();
+  if (!a.partial || !a.slot_clock) return RCABEAM_ERROR_CUDA;
   const int items = a.ntiles * a.chunks;
   const unsigned grid = unsigned(std::min(std::min(items, sms), tc::kMaxCtas));
   kern<<<grid, tc::threads_for(stages), smem>>>(mh[0], mh[1], ml[0], ml[1], a);
