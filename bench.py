@@ -43,9 +43,10 @@ FS, FD, C = 20e6, 15e6, 1540.0
 T_START = 4e-6
 RANK_START = 3
 # DRAM bytes (read + write) per unit of the bf16x3 tensor-core DAS launch,
-# from one ncu capture: 1609.3 MB for 65,536 voxels x 256 ch x 11 ang x 104 frm
-# (the 512-step segment partial sums account for most of the writes).
-DAS_DRAM_BYTES_PER_UNIT = 1609.26e6 / (65536 * 256 * 11 * 104)
+# from one ncu capture on the central 64 x 128 x 64 block at 200 frames
+# (8192 work items): 43.96 GB read + 5.22 GB written for
+# 524,288 voxels x 256 ch x 11 ang x 200 frm.
+DAS_DRAM_BYTES_PER_UNIT = (43.956e9 + 5.215e9) / (524288 * 256 * 11 * 200)
 
 
 SUBGRID = None  # (nx, nz, ny) central block of the full grid, same spacing (profiling)
@@ -264,8 +265,8 @@ def run_b200(args, rank: int, world: int) -> dict | None:
                      "frac": round(mma_flops / das_s / 1e12 / tensor_peak, 4), "peak_source": peak_source,
                      "traffic": round(DAS_DRAM_BYTES_PER_UNIT * units),
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one opw_tc launch on the "
-                                       "central 32x64x32 block (104 frames), scaled by units "
-                                       "(profiles/opw_tc_bf16x3_central_block_ncu.md)",
+                                       "central 64x128x64 block (200 frames), scaled by units "
+                                       "(profiles/opw_tc_bf16x3_central_blocks_200frames_ncu.md)",
                      "das_ms": ch["das_ms"],
                      "note": "dense tcgen05 MMA flops issued per launch (2 groups x 3 products x M128 x N(2 x pass "
                              f"frames {pass_frames}) x K16 per 128-voxel tile step) vs "
