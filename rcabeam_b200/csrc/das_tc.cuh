@@ -115,6 +115,8 @@ struct Args {
   int* err;
 };
 
+constexpr int kCtrlBytes = 512;  // barriers, stage tags, counters, TMEM slot
+
 template <bool BF16X3>
 struct Layout {
   static constexpr int kPlanes = BF16X3 ? 2 : 1;
@@ -122,11 +124,12 @@ struct Layout {
   __host__ __device__ static size_t stage_bytes(int nbox) {
     return 4 * kAMatBytes + size_t(kPlanes) * nbox * kBoxBytes;
   }
-  // stages | control (barriers, meta, counter, TMEM slot) | angle table |
-  // per-tile transmit delays [2][na][128] double | transmit phases [2][na][128] float2
+  // stages | control (barriers, meta, counters, TMEM slot) | angle table [na][3] double |
+  // per-tile transmit delay bases [2][na] double, offsets [2][na][128] float and
+  // phases [2][na][128] float2 (the caller adds up to 1 KB to align the base).
   static size_t bytes(int nbox, int na, int stages) {
-    return size_t(stages) * stage_bytes(nbox) + 1024 + size_t(na) * 3 * sizeof(double) + size_t(na) * 2 * kVox * 16 +
-           1024;
+    return size_t(stages) * stage_bytes(nbox) + kCtrlBytes + size_t(na) * 5 * sizeof(double) +
+           size_t(na) * 2 * kVox * (sizeof(float) + sizeof(float2));
   }
 };
 
@@ -348,9 +351,14 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
   int* item_steps = counter + 1;                         // steps staged for the current item
   volatile int* acc_kind = item_steps + 1;               // AccKind of the pending flush
   int* walk_start = item_steps + 2;                      // first channel slot of the current item
-  double* angle_tab = reinterpret_cast<double*>(ctrl + 1024);
-  double* tx_delay = angle_tab + 3 * p.na;                                   // [2][na][128]
-  float2* tx_phase = reinterpret_cast<float2*>(tx_delay + 2 * p.na * kVox);  // [2][na][128]
+  double* angle_tab = reinterpret_cast<double*>(ctrl + kCtrlBytes);
+  // Transmit delay of (aperture, angle, voxel) = tx_base[aperture, angle] (the
+  // tile's first voxel, float64) + tx_off (float: within a compact tile the
+  // offsets stay below a few hundred ns, so float keeps them to ~1e-14 s); the
+  // halved table is what lets a sixth ring stage fit beside 3xBF16 stages.
+  double* tx_base = angle_tab + 3 * p.na;                                  // [2][na]
+  float* tx_off = reinterpret_cast<float*>(tx_base + 2 * p.na);            // [2][na][128]
+  float2* tx_phase = reinterpret_cast<float2*>(tx_off + 2 * p.na * kVox);  // [2][na][128]
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -456,6 +464,10 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
       }
       // Per-tile transmit table, filled cooperatively by the builder warps.
       builders_sync();  // previous item's table reads are complete
+      // The tile's first slot always holds a voxel (tiles are filled in order).
+      const size_t q0 = size_t(tile) * kVox;
+      const size_t r3 = 3 * size_t(p.order ? p.order[q0] : unsigned(q0));
+      const double x0 = double(p.scan[r3]), z0 = double(p.scan[r3 + 1]), y0 = double(p.scan[r3 + 2]);
       for (int e = warp * 32 + lane; e < 2 * p.na * kVox; e += kBuilders * 32) {
         const int v = e % kVox, ca = e / kVox, config = ca / p.na, a = ca % p.na;
         const size_t q = size_t(tile) * kVox + v;
@@ -465,7 +477,9 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
         const double z = vid != UINT_MAX ? double(p.scan[b3 + 1]) : 0.0;
         const double y = vid != UINT_MAX ? double(p.scan[b3 + 2]) : 0.0;
         const double ttx = transmit_delay(config ? x : y, z, angle_tab[3 * a], angle_tab[3 * a + 1], p.c);
-        tx_delay[e] = ttx;
+        const double ref = transmit_delay(config ? x0 : y0, z0, angle_tab[3 * a], angle_tab[3 * a + 1], p.c);
+        tx_off[e] = float(ttx - ref);
+        if (v == 0) tx_base[ca] = ref;
         tx_phase[e] = demod_phase(p.fd, ttx);
       }
       // Channel slots u = aperture * nc + channel are walked from the slot the
@@ -495,13 +509,15 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
           }
           for (int a = 0; a < p.na; ++a) {
             const double start = angle_tab[3 * a + 2];
+            const double base_tx = tx_base[config * p.na + a];
             int i0[4];
             float w[4];
             int lo = INT_MAX, hi = -1;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
               const int ti = (config * p.na + a) * kVox + lane + 32 * j;
-              const double sample = __dmul_rn(__dadd_rn(__dadd_rn(tx_delay[ti], trx[j]), -start), p.fs);
+              const double ttx = __dadd_rn(base_tx, double(tx_off[ti]));
+              const double sample = __dmul_rn(__dadd_rn(__dadd_rn(ttx, trx[j]), -start), p.fs);
               const bool in_window = act[j] && sample >= 0.0 && sample <= double(p.ns - 1);
               const double fl = floor(sample);
               i0[j] = in_window ? int(fl) : -1;
