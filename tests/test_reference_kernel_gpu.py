@@ -405,3 +405,46 @@ def test_full_workload_against_reference_kernels(ref):
     assert err <= TOL
     assert rows["b200 bf16x2 (tcgen05, 3 products)"] < rows["reference float32"]
     assert rows["b200 float16 (tcgen05)"] < rows["reference float16"]
+
+
+def test_st_sw_block_against_reference_kernels(ref):
+    """St-SW k = 2 on the central 32 x 64 x 32 block of the full workload (IQ 512x128x11x200): both
+    libraries through the C ABI in 4096-voxel tiles with a k^2 nt series workspace (the reference
+    binding's tiling, python.cpp:553-565); power agreement and both times (printed)."""
+    ns, nc, na, nt, k = 512, 128, 11, 200, 2
+    el = (np.arange(nc) - (nc - 1) / 2) * 0.11e-3
+    half = (nc - 1) / 2 * 0.11e-3
+    axes = (np.linspace(-half, half, 128), np.linspace(4e-3, 12e-3, 256), np.linspace(-half, half, 128))
+    grid = tuple(a[(len(a) - n) // 2:(len(a) - n) // 2 + n] for a, n in zip(axes, (32, 64, 32)))
+    angles = np.deg2rad(np.linspace(-10, 10, na))
+    gen = torch.Generator(device="cuda").manual_seed(9)
+    case = Case.__new__(Case)
+    case.ns, case.nc, case.na, case.nt = ns, nc, na, nt
+    scan = scan_coords(grid)
+    case.nv = len(scan)
+    f32 = lambda v: _d(np.asarray(v, np.float32))  # noqa: E731
+    case.scan, case.xe, case.ye, case.angles = f32(scan), f32(el), f32(el), f32(angles)
+    case.starts = f32(np.full(na, 4e-6))
+    case.consts = (1540.0, 20e6, 15e6, -1.0)
+    shape = (ns, nc, na, nt)
+    case.drc = torch.complex(torch.randn(shape, generator=gen, device="cuda"),
+                             torch.randn(shape, generator=gen, device="cuda"))
+    case.dcr = torch.complex(torch.randn(shape, generator=gen, device="cuda"),
+                             torch.randn(shape, generator=gen, device="cuda"))
+    units = case.nv * 2 * nc * na * nt
+    results = {}
+    for name, handle in (("reference", ref), ("b200", _lib.lib())):
+        case.stsw(handle, k)  # warm-up (includes packing)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        pd, w = case.stsw(handle, k)
+        b.record()
+        torch.cuda.synchronize()
+        results[name] = (a.elapsed_time(b), pd * w / w.max())
+    err = rel_l2(results["b200"][1], results["reference"][1])
+    print(f"\nSt-SW k={k}, {case.nv} voxels, IQ {shape}, packing + series + finish, 4096-voxel tiles:")
+    for name, (ms, _) in results.items():
+        print(f"  {name:10s} {ms:9.1f} ms  {units / ms / 1e6:8.1f} Gsamples/s")
+    print(f"  St-SW power rel. L2 b200 vs reference: {err:.2e}")
+    assert err <= 1e-3
