@@ -44,9 +44,9 @@ T_START = 4e-6
 RANK_START = 3
 # DRAM bytes (read + write) per unit of the bf16x3 tensor-core DAS launch,
 # from one ncu capture on the central 64 x 128 x 64 block at 200 frames
-# (8192 work items): 43.96 GB read + 5.22 GB written for
+# (8192 work items): 45.09 GB read + 5.22 GB written for
 # 524,288 voxels x 256 ch x 11 ang x 200 frm.
-DAS_DRAM_BYTES_PER_UNIT = (43.956e9 + 5.215e9) / (524288 * 256 * 11 * 200)
+DAS_DRAM_BYTES_PER_UNIT = (45.085e9 + 5.220e9) / (524288 * 256 * 11 * 200)
 
 
 SUBGRID = None  # (nx, nz, ny) central block of the full grid, same spacing (profiling)
