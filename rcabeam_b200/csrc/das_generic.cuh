@@ -220,17 +220,36 @@ __global__ void __launch_bounds__(kWarps * 32) stsw_series(das::Args p, float2* 
   const Voxel q = load_voxel(p.scan, v);
   const float2* rc = static_cast<const float2*>(p.rc);
   const float2* cr = static_cast<const float2*>(p.cr);
+  __shared__ __align__(16) Tap taps[kWarps][2][32];
+  Tap* tap_rc = taps[threadIdx.x >> 5][0];
+  Tap* tap_cr = taps[threadIdx.x >> 5][1];
   float2 r[RF] = {}, s[RF] = {};
   float2 mr[K][RF] = {}, mq[K][RF] = {};
   float vr[K][RF] = {}, vq[K][RF] = {};
   for (int a = 0; a < p.na; ++a) {
     float2 ar[RF] = {}, aq[RF] = {};
+    // The angle's transmit delays of this voxel, once per angle (the same float64
+    // operations as tap_of, so the taps are unchanged).
+    const double th = double(p.angles[a]), cs = cos(th), sn = sin(th), start = double(p.starts[a]);
+    const double ttx_rc = transmit_delay(q.y, q.z, cs, sn, p.c), ttx_cr = transmit_delay(q.x, q.z, cs, sn, p.c);
+    auto tap = [&](int config, int c0) -> Tap {
+      const int ch = c0 + lane;
+      if (ch >= p.nc) return Tap{-1, 0.f, make_float2(0.f, 0.f)};
+      bool act;
+      const double trx = receive_delay(config ? q.y : q.x, q.z, double((config ? p.ye : p.xe)[ch]), p.c, p.fn, &act);
+      return make_tap(__dadd_rn(config ? ttx_cr : ttx_rc, trx), start, p.fs, p.fd, p.ns, act);
+    };
     for (int c0 = 0; c0 < p.nc; c0 += 32) {
-      const Tap lr = lane_tap(p, q, 0, true, a, c0), lq = lane_tap(p, q, 1, true, a, c0);
+      // Each lane forms one channel's taps; the warp then reads them back from
+      // shared memory (one broadcast 16-byte load per tap instead of four shuffles).
+      __syncwarp();  // the previous chunk's reads are done
+      tap_rc[lane] = tap(0, c0);
+      tap_cr[lane] = tap(1, c0);
+      __syncwarp();
       const int count = min(32, p.nc - c0);
       for (int j = 0; j < count; ++j) {
         const int ch = c0 + j;
-        const Tap tr = shfl_tap(lr, j), tq = shfl_tap(lq, j);
+        const Tap tr = tap_rc[j], tq = tap_cr[j];
 #pragma unroll
         for (int f = 0; f < RF; ++f) {
           const int frame = fbase + 32 * f;
