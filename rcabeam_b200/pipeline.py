@@ -204,6 +204,39 @@ class FilteredOpw:
         self.host_power.copy_(self.power, non_blocking=True)
         return self.host_power
 
+    def run_host_sequence(self, pairs, outputs=None) -> list[torch.Tensor]:
+        """Filtered power of a sequence of pinned host ``(rc, cr)`` ensembles, each uploaded,
+        reconstructed and read back (pinned float64 host arrays, one per ensemble).
+
+        Each ensemble's upload runs on a side stream as soon as the previous ensemble no
+        longer reads the raw channels (after packing; after filtering in the channel
+        domain), so it overlaps that ensemble's reconstruction, the way an acquisition
+        stream feeds the pipeline.  ``outputs`` may pass preallocated pinned arrays.
+        """
+        pairs = list(pairs)
+        if outputs is None:
+            outputs = [torch.empty(self.nv, dtype=torch.float64, pin_memory=True) for _ in pairs]
+        if len(outputs) != len(pairs):
+            raise ValueError("one output per ensemble is required")
+        if not hasattr(self, "_copy_stream"):
+            self._copy_stream = torch.cuda.Stream(self.device)
+            self._uploaded = torch.cuda.Event()
+        # Raw channels are last read by the packing (beamformed) or the filter (channel domain).
+        consumed = self.events[3] if self.domain == "channel" else self.events[1]
+        main = torch.cuda.current_stream(self.device)
+        self._copy_stream.wait_stream(main)  # no upload before the work already queued
+        for (rc_host, cr_host), out in zip(pairs, outputs):
+            with torch.cuda.stream(self._copy_stream):
+                self._copy_stream.wait_event(consumed)
+                self.inputs[0].copy_(rc_host, non_blocking=True)
+                self.inputs[1].copy_(cr_host, non_blocking=True)
+                self._uploaded.record(self._copy_stream)
+            main.wait_event(self._uploaded)
+            self.run(self.inputs[0], self.inputs[1])
+            out.copy_(self.power.view(-1), non_blocking=True)
+        torch.cuda.synchronize(self.device)
+        return outputs
+
     @staticmethod
     def collect_das_ms(pair) -> float:
         return pair[0].elapsed_time(pair[1])

@@ -210,3 +210,25 @@ def test_filtered_pipeline_matches_fp64_oracle():
     host = plan.run_host(torch.from_numpy(rc).pin_memory(), torch.from_numpy(cr).pin_memory())
     plan.check()
     assert rel_l2(host.numpy().reshape(6, 10, 5), expected) < 1e-4
+
+
+@pytest.mark.parametrize("storage,precision,domain", [("float32", "complex128", "beamformed"),
+                                                      ("bf16x2", "bf16x3", "beamformed"),
+                                                      ("bf16x2", "bf16x3", "channel")])
+def test_host_sequence_matches_single_runs(storage, precision, domain):
+    """run_host_sequence (uploads overlapping the previous ensemble's reconstruction) returns, for
+    three different ensembles in a row, the powers of separate runs (1e-6: the tensor-core DAS sums
+    in an order that depends on timing)."""
+    scenes = [_scene(seed=s) for s in (5, 6, 7)]
+    _, _, angles, t0, grid, geom = scenes[0]
+    plan = pipeline.FilteredOpw(scenes[0][0].shape, angles, t0, grid, geom, rank_start=3, precision=precision,
+                                iq_storage=storage, domain=domain)
+    single = [plan.run(_dev(rc), _dev(cr)).cpu().numpy().ravel() for rc, cr, *_ in scenes]
+    pairs = [(torch.from_numpy(rc).pin_memory(), torch.from_numpy(cr).pin_memory()) for rc, cr, *_ in scenes]
+    outs = plan.run_host_sequence(pairs)
+    plan.check()
+    assert len(outs) == 3
+    for got, want in zip(outs, single):
+        assert rel_l2(got.numpy(), want) <= 1e-6
+    with pytest.raises(ValueError, match="one output"):
+        plan.run_host_sequence(pairs, outputs=outs[:2])
