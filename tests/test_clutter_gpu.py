@@ -217,8 +217,10 @@ def test_filtered_pipeline_matches_fp64_oracle():
                                                       ("bf16x2", "bf16x3", "channel")])
 def test_host_sequence_matches_single_runs(storage, precision, domain):
     """run_host_sequence (uploads overlapping the previous ensemble's reconstruction) returns, for
-    three different ensembles in a row, the powers of separate runs (1e-6: the tensor-core DAS sums
-    in an order that depends on timing)."""
+    three different ensembles in a row, the powers of separate runs.  The SIMT path is deterministic;
+    the tensor-core DAS starts each item's channel walk where the other CTAs are, so its float32 sums
+    run in a timing-dependent order (~1e-7 of the IQ), which removing the 100x stronger tissue
+    signal amplifies in the filtered power: 5e-5, under the 1e-4 bar of the filtered pipeline."""
     scenes = [_scene(seed=s) for s in (5, 6, 7)]
     _, _, angles, t0, grid, geom = scenes[0]
     plan = pipeline.FilteredOpw(scenes[0][0].shape, angles, t0, grid, geom, rank_start=3, precision=precision,
@@ -228,7 +230,8 @@ def test_host_sequence_matches_single_runs(storage, precision, domain):
     outs = plan.run_host_sequence(pairs)
     plan.check()
     assert len(outs) == 3
+    tol = 1e-12 if storage == "float32" else 5e-5
     for got, want in zip(outs, single):
-        assert rel_l2(got.numpy(), want) <= 1e-6
+        assert rel_l2(got.numpy(), want) <= tol
     with pytest.raises(ValueError, match="one output"):
         plan.run_host_sequence(pairs, outputs=outs[:2])
