@@ -102,14 +102,21 @@ class FilteredOpw:
         if self.k:
             torch.index_select(vt, 0, ranks, out=self.vectors[: self.k])
 
-    def run(self, rc: torch.Tensor, cr: torch.Tensor) -> torch.Tensor:
-        """Filtered power of resident complex64 RC/CR channels ``(ns, nc, na, nt)``."""
+    def run(self, rc: torch.Tensor, cr: torch.Tensor, after_inputs=None) -> torch.Tensor:
+        """Filtered power of resident complex64 RC/CR channels ``(ns, nc, na, nt)``.
+
+        ``after_inputs`` (optional) is called once the work that reads ``rc`` / ``cr`` has
+        been queued (packing; in the channel domain, filtering), before the rest of the
+        step: a caller may queue the next ensemble's upload into them there.
+        """
         if self.domain == "channel":
-            return self._run_channel(rc, cr)
+            return self._run_channel(rc, cr, after_inputs)
         ev = self.events
         ev[0].record()
         self._pack(rc, cr)
         ev[1].record()
+        if after_inputs is not None:
+            after_inputs()
         self._das(self.iq)
         ev[2].record()
         self.gram.accumulate((self.iq,), self.precision, self.group)
@@ -126,7 +133,7 @@ class FilteredOpw:
         self.last_das_event_ms = (ev[1], ev[2])
         return self.power.view(self.shape)
 
-    def _run_channel(self, rc: torch.Tensor, cr: torch.Tensor) -> torch.Tensor:
+    def _run_channel(self, rc: torch.Tensor, cr: torch.Tensor, after_inputs=None) -> torch.Tensor:
         """Channel domain: shared basis of the RC and CR channel rows, filter, pack, OPW power."""
         ns, nc, na, nt = self.channel_shape
         ev = self.events
@@ -142,6 +149,8 @@ class FilteredOpw:
                 _lib.call("rcabeam_project_device", src.data_ptr(), dst.data_ptr(), None, rows, nt, 0,
                           self.vectors.data_ptr(), self.k, (1 if self.subtract else 0) | 2)
         ev[3].record()
+        if after_inputs is not None:
+            after_inputs()
         if self.rank[0] == self.rank[1]:
             self.power.zero_()
             for e in ev[4:]:
@@ -225,14 +234,23 @@ class FilteredOpw:
         consumed = self.events[3] if self.domain == "channel" else self.events[1]
         main = torch.cuda.current_stream(self.device)
         self._copy_stream.wait_stream(main)  # no upload before the work already queued
-        for (rc_host, cr_host), out in zip(pairs, outputs):
+
+        def upload(i: int) -> None:
+            rc_host, cr_host = pairs[i]
             with torch.cuda.stream(self._copy_stream):
                 self._copy_stream.wait_event(consumed)
                 self.inputs[0].copy_(rc_host, non_blocking=True)
                 self.inputs[1].copy_(cr_host, non_blocking=True)
                 self._uploaded.record(self._copy_stream)
+
+        if pairs:
+            upload(0)
+        for i, out in enumerate(outputs):
             main.wait_event(self._uploaded)
-            self.run(self.inputs[0], self.inputs[1])
+            # The next upload is queued as soon as this step's reads of the inputs are queued,
+            # i.e. before the step's later stages (whose eigensolver may block the host).
+            nxt = (lambda j=i + 1: upload(j)) if i + 1 < len(pairs) else None
+            self.run(self.inputs[0], self.inputs[1], after_inputs=nxt)
             out.copy_(self.power.view(-1), non_blocking=True)
         torch.cuda.synchronize(self.device)
         return outputs
