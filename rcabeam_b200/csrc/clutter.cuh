@@ -54,6 +54,33 @@ __global__ void max_abs_kernel(const IN* x, size_t n, unsigned long long* out) {
   if ((threadIdx.x & 31) == 0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(m)));
 }
 
+// Complex64 max |component| at HBM speed: float4 loads (two samples), four in
+// flight per thread; the float maximum is exact, so the result equals
+// max_abs_kernel's.  x must be 16-byte aligned; an odd last sample is read alone.
+__global__ void __launch_bounds__(256) max_abs_c64(const float2* __restrict__ x, size_t n,
+                                                   unsigned long long* out) {
+  const float4* x4 = reinterpret_cast<const float4*>(x);
+  const size_t n4 = n / 2, stride = size_t(gridDim.x) * blockDim.x;
+  size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  float m = 0.f;
+  auto fold = [&m](float4 v) { m = fmaxf(fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y))), fmaxf(fabsf(v.z), fabsf(v.w))); };
+  for (; i + 3 * stride < n4; i += 4 * stride) {
+    const float4 a = __ldg(x4 + i), b = __ldg(x4 + i + stride), c = __ldg(x4 + i + 2 * stride),
+                 d = __ldg(x4 + i + 3 * stride);
+    fold(a);
+    fold(b);
+    fold(c);
+    fold(d);
+  }
+  for (; i < n4; i += stride) fold(__ldg(x4 + i));
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+    const float2 t = x[n - 1];
+    m = fmaxf(m, fmaxf(fabsf(t.x), fabsf(t.y)));
+  }
+  for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(double(m))));
+}
+
 // Partial Gram of one upper-triangle tile (bi <= bj) over a slice of rows.
 // Each thread owns a 4 x 4 block of complex outputs; rows are staged through
 // shared memory already scaled and converted to the accumulation type.

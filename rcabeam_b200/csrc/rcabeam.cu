@@ -650,8 +650,16 @@ rcabeam_status rcabeam_clutter_scale_device(const void* iq, size_t n, int comple
   auto* out = reinterpret_cast<unsigned long long*>(scale);
   if (complex128)
     clutter::max_abs_kernel<double2><<<296, 256>>>(static_cast<const double2*>(iq), n, out);
-  else
+  else if (reinterpret_cast<uintptr_t>(iq) % 16 == 0) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t want = (n / 2 + 4 * 256 - 1) / (4 * 256);  // four float4 per thread
+    const unsigned blocks = unsigned(std::max<size_t>(1, std::min<size_t>(want, size_t(sms) * 8)));
+    clutter::max_abs_c64<<<blocks, 256>>>(static_cast<const float2*>(iq), n, out);
+  } else {
     clutter::max_abs_kernel<float2><<<296, 256>>>(static_cast<const float2*>(iq), n, out);
+  }
   return launch_status();
 }
 

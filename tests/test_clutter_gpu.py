@@ -235,3 +235,18 @@ def test_host_sequence_matches_single_runs(storage, precision, domain):
         assert rel_l2(got.numpy(), want) <= tol
     with pytest.raises(ValueError, match="one output"):
         plan.run_host_sequence(pairs, outputs=outs[:2])
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 4096, 1_000_003])
+@pytest.mark.parametrize("offset", [0, 1])
+def test_scale_max_abs_matches_torch(n, offset):
+    """rcabeam_clutter_scale_device on complex64 (vectorized path for 16-byte aligned data, the
+    scalar path for an 8-byte offset) equals max |re|, |im| exactly, odd lengths included."""
+    g = torch.Generator(device="cuda").manual_seed(n)
+    buf = torch.randn((n + 1) * 2, generator=g, device="cuda", dtype=torch.float32)
+    buf[2 * offset + 2 * (n - 1) + 1] = 7.5  # the largest component sits in the last sample
+    x = torch.view_as_complex(buf.view(-1, 2))[offset:offset + n]
+    scale = torch.zeros(1, dtype=torch.float64, device="cuda")
+    _lib.call("rcabeam_clutter_scale_device", x.data_ptr(), n, 0, scale.data_ptr())
+    want = torch.view_as_real(x).abs().max().double()
+    assert float(scale.item()) == float(want.item()) == 7.5
