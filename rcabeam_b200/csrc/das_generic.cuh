@@ -13,7 +13,10 @@
 namespace rcb {
 namespace generic {
 
-constexpr int kRegFrames = 4;
+// One register frame per lane: these warp-per-voxel kernels are bound by the
+// latency of their per-frame gathers, so resident warps matter more than the
+// taps each 32-frame block re-forms (St-SW, k = 2: 205 ms at 4 frames, 97 ms at 1).
+constexpr int kRegFrames = 1;
 constexpr int kWarps = 4;
 
 struct Voxel {
@@ -43,6 +46,26 @@ __device__ __forceinline__ float2 packed_sample(const float2* iq, const Tap& t, 
   float2 va = iq[idx], vb = iq[nxt];
   float2 val = make_float2(fmaf(t.w, vb.x - va.x, va.x), fmaf(t.w, vb.y - va.y, va.y));
   return cmul(val, t.phase);
+}
+
+// Transmit delays of a voxel for one angle (RC transmits along y, CR along x),
+// formed once per angle with the float64 operations of tap_of.
+struct AngleTx {
+  double rc, cr, start;
+};
+__device__ __forceinline__ AngleTx angle_tx(const das::Args& p, const Voxel& q, int a) {
+  const double th = double(p.angles[a]), cs = cos(th), sn = sin(th);
+  return AngleTx{transmit_delay(q.y, q.z, cs, sn, p.c), transmit_delay(q.x, q.z, cs, sn, p.c), double(p.starts[a])};
+}
+
+// Tap of channel c0 + lane for one aperture (empty beyond nc): tap_of's float64
+// operations with the angle's transmit delay precomputed (identical taps).
+__device__ __forceinline__ Tap lane_tap_tx(const das::Args& p, const Voxel& q, int config, int c0, const AngleTx& tx) {
+  const int ch = c0 + int(threadIdx.x & 31);
+  if (ch >= p.nc) return Tap{-1, 0.f, make_float2(0.f, 0.f)};
+  bool act;
+  const double trx = receive_delay(config ? q.y : q.x, q.z, double((config ? p.ye : p.xe)[ch]), p.c, p.fn, &act);
+  return make_tap(__dadd_rn(config ? tx.cr : tx.rc, trx), tx.start, p.fs, p.fd, p.ns, act);
 }
 
 __device__ __forceinline__ Tap shfl_tap(const Tap& t, int src) {
@@ -80,14 +103,22 @@ __device__ void nonlinear_voxel(const das::Args& p, size_t v, int fblock) {
   if constexpr (METHOD == 2) {
     // RC-FMAS: sum over angles of signed square roots of channel sums, RC * CR.
     float2 r[kRegFrames] = {}, s[kRegFrames] = {};
+    // Each lane forms one channel's taps; the warp reads them back from shared memory.
+    __shared__ __align__(16) Tap taps[kWarps][2][32];
+    Tap* tap_rc = taps[threadIdx.x >> 5][0];
+    Tap* tap_cr = taps[threadIdx.x >> 5][1];
     for (int a = 0; a < p.na; ++a) {
       float2 ar[kRegFrames] = {}, aq[kRegFrames] = {};
+      const AngleTx tx = angle_tx(p, q, a);
       for (int c0 = 0; c0 < p.nc; c0 += 32) {
-        const Tap lr = lane_tap(p, q, 0, true, a, c0), lq = lane_tap(p, q, 1, true, a, c0);
+        __syncwarp();  // the previous chunk's reads are done
+        tap_rc[lane] = lane_tap_tx(p, q, 0, c0, tx);
+        tap_cr[lane] = lane_tap_tx(p, q, 1, c0, tx);
+        __syncwarp();
         const int count = min(32, p.nc - c0);
         for (int j = 0; j < count; ++j) {
           const int ch = c0 + j;
-          const Tap tr = shfl_tap(lr, j), tq = shfl_tap(lq, j);
+          const Tap tr = tap_rc[j], tq = tap_cr[j];
 #pragma unroll
           for (int f = 0; f < kRegFrames; ++f) {
             int frame = fbase + 32 * f;
@@ -228,23 +259,13 @@ __global__ void __launch_bounds__(kWarps * 32) stsw_series(das::Args p, float2* 
   float vr[K][RF] = {}, vq[K][RF] = {};
   for (int a = 0; a < p.na; ++a) {
     float2 ar[RF] = {}, aq[RF] = {};
-    // The angle's transmit delays of this voxel, once per angle (the same float64
-    // operations as tap_of, so the taps are unchanged).
-    const double th = double(p.angles[a]), cs = cos(th), sn = sin(th), start = double(p.starts[a]);
-    const double ttx_rc = transmit_delay(q.y, q.z, cs, sn, p.c), ttx_cr = transmit_delay(q.x, q.z, cs, sn, p.c);
-    auto tap = [&](int config, int c0) -> Tap {
-      const int ch = c0 + lane;
-      if (ch >= p.nc) return Tap{-1, 0.f, make_float2(0.f, 0.f)};
-      bool act;
-      const double trx = receive_delay(config ? q.y : q.x, q.z, double((config ? p.ye : p.xe)[ch]), p.c, p.fn, &act);
-      return make_tap(__dadd_rn(config ? ttx_cr : ttx_rc, trx), start, p.fs, p.fd, p.ns, act);
-    };
+    const AngleTx tx = angle_tx(p, q, a);  // the voxel's transmit delays, once per angle
     for (int c0 = 0; c0 < p.nc; c0 += 32) {
       // Each lane forms one channel's taps; the warp then reads them back from
       // shared memory (one broadcast 16-byte load per tap instead of four shuffles).
       __syncwarp();  // the previous chunk's reads are done
-      tap_rc[lane] = tap(0, c0);
-      tap_cr[lane] = tap(1, c0);
+      tap_rc[lane] = lane_tap_tx(p, q, 0, c0, tx);
+      tap_cr[lane] = lane_tap_tx(p, q, 1, c0, tx);
       __syncwarp();
       const int count = min(32, p.nc - c0);
       for (int j = 0; j < count; ++j) {

@@ -419,7 +419,7 @@ static rcabeam_status ensemble_impl(const void* rc, const void* cr, const float*
   if (method == 4) {
     // St-SW: series into the caller's workspace (nv k^2 nt complex64), then
     // energies, pair sums, raw weights and the XDoppler magnitude.
-    constexpr int kStswFrames = 1;
+    constexpr int kStswFrames = generic::kRegFrames;
     const unsigned blocks = unsigned((nv + generic::kWarps - 1) / generic::kWarps);
     dim3 grid(blocks, unsigned((nt + 32 * kStswFrames - 1) / (32 * kStswFrames)));
     float2* series = static_cast<float2*>(workspace);

@@ -407,11 +407,9 @@ def test_full_workload_against_reference_kernels(ref):
     assert rows["b200 float16 (tcgen05)"] < rows["reference float16"]
 
 
-def test_st_sw_block_against_reference_kernels(ref):
-    """St-SW k = 2 on the central 32 x 64 x 32 block of the full workload (IQ 512x128x11x200): both
-    libraries through the C ABI in 4096-voxel tiles with a k^2 nt series workspace (the reference
-    binding's tiling, python.cpp:553-565); power agreement and both times (printed)."""
-    ns, nc, na, nt, k = 512, 128, 11, 200, 2
+def _full_block_case():
+    """The full workload's channels (IQ 512x128x11x200) on its central 32 x 64 x 32 voxel block."""
+    ns, nc, na, nt = 512, 128, 11, 200
     el = (np.arange(nc) - (nc - 1) / 2) * 0.11e-3
     half = (nc - 1) / 2 * 0.11e-3
     axes = (np.linspace(-half, half, 128), np.linspace(4e-3, 12e-3, 256), np.linspace(-half, half, 128))
@@ -431,7 +429,16 @@ def test_st_sw_block_against_reference_kernels(ref):
                              torch.randn(shape, generator=gen, device="cuda"))
     case.dcr = torch.complex(torch.randn(shape, generator=gen, device="cuda"),
                              torch.randn(shape, generator=gen, device="cuda"))
-    units = case.nv * 2 * nc * na * nt
+    return case
+
+
+def test_st_sw_block_against_reference_kernels(ref):
+    """St-SW k = 2 on the central block of the full workload: both libraries through the C ABI in
+    4096-voxel tiles with a k^2 nt series workspace (the reference binding's tiling,
+    python.cpp:553-565); power agreement and both times (printed)."""
+    case, k = _full_block_case(), 2
+    shape = (case.ns, case.nc, case.na, case.nt)
+    units = case.nv * 2 * case.nc * case.na * case.nt
     results = {}
     for name, handle in (("reference", ref), ("b200", _lib.lib())):
         case.stsw(handle, k)  # warm-up (includes packing)
@@ -448,3 +455,26 @@ def test_st_sw_block_against_reference_kernels(ref):
         print(f"  {name:10s} {ms:9.1f} ms  {units / ms / 1e6:8.1f} Gsamples/s")
     print(f"  St-SW power rel. L2 b200 vs reference: {err:.2e}")
     assert err <= 1e-3
+
+
+def test_rc_fmas_block_against_reference_kernels(ref):
+    """RC-FMAS (method 2) on the central block of the full workload, signal and power written, both
+    libraries in the reference binding's 4096-voxel tiles: agreement and both times (printed)."""
+    case = _full_block_case()
+    units = case.nv * 2 * case.nc * case.na * case.nt
+    results = {}
+    for name, handle in (("reference", ref), ("b200", _lib.lib())):
+        packed = case.packed(handle)
+        case.ensemble(handle, method=2, packed=packed)  # warm-up
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        pd, sig = case.ensemble(handle, method=2, packed=packed)
+        b.record()
+        torch.cuda.synchronize()
+        results[name] = (a.elapsed_time(b), pd, sig)
+    print(f"\nRC-FMAS, {case.nv} voxels, IQ {(case.ns, case.nc, case.na, case.nt)}, signal + power, 4096-voxel tiles:")
+    for name, (ms, *_) in results.items():
+        print(f"  {name:10s} {ms:9.1f} ms  {units / ms / 1e6:8.1f} Gsamples/s")
+    assert rel_l2(results["b200"][1], results["reference"][1]) <= TOL
+    assert rel_l2(results["b200"][2], results["reference"][2]) <= TOL
