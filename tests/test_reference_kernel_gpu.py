@@ -457,23 +457,26 @@ def test_st_sw_block_against_reference_kernels(ref):
     assert err <= 1e-3
 
 
-def test_rc_fmas_block_against_reference_kernels(ref):
-    """RC-FMAS (method 2) on the central block of the full workload, signal and power written, both
-    libraries in the reference binding's 4096-voxel tiles: agreement and both times (printed)."""
+@pytest.mark.parametrize("method,label", [(2, "RC-FMAS"), (3, "DMAS-CCF-ACF")])
+def test_nonlinear_block_against_reference_kernels(ref, method, label):
+    """RC-FMAS (method 2) and DMAS-CCF-ACF (method 3) on the central block of the full workload,
+    signal and power written, both libraries in the reference binding's 4096-voxel tiles:
+    agreement and both times (printed)."""
     case = _full_block_case()
     units = case.nv * 2 * case.nc * case.na * case.nt
     results = {}
     for name, handle in (("reference", ref), ("b200", _lib.lib())):
         packed = case.packed(handle)
-        case.ensemble(handle, method=2, packed=packed)  # warm-up
+        case.ensemble(handle, method=method, packed=packed)  # warm-up
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        pd, sig = case.ensemble(handle, method=2, packed=packed)
+        pd, sig = case.ensemble(handle, method=method, packed=packed)
         b.record()
         torch.cuda.synchronize()
         results[name] = (a.elapsed_time(b), pd, sig)
-    print(f"\nRC-FMAS, {case.nv} voxels, IQ {(case.ns, case.nc, case.na, case.nt)}, signal + power, 4096-voxel tiles:")
+    print(f"\n{label}, {case.nv} voxels, IQ {(case.ns, case.nc, case.na, case.nt)}, signal + power, "
+          "4096-voxel tiles:")
     for name, (ms, *_) in results.items():
         print(f"  {name:10s} {ms:9.1f} ms  {units / ms / 1e6:8.1f} Gsamples/s")
     assert rel_l2(results["b200"][1], results["reference"][1]) <= TOL
