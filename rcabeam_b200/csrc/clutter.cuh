@@ -205,10 +205,12 @@ __global__ void __launch_bounds__(256)
           }
         }
       }
+      if (c0 + c < k) {  // k is uniform over the warp: slots past k reduce nothing
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        yr += __shfl_xor_sync(0xffffffffu, yr, off);
-        yi += __shfl_xor_sync(0xffffffffu, yi, off);
+        for (int off = 16; off > 0; off >>= 1) {
+          yr += __shfl_xor_sync(0xffffffffu, yr, off);
+          yi += __shfl_xor_sync(0xffffffffu, yi, off);
+        }
       }
       y[c] = make_double2(yr, yi);
       retained += yr * yr + yi * yi;
