@@ -259,5 +259,89 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+constexpr int kProjSmall = 4;  // vectors of the single-chunk form
+
+// Single-chunk form of project_rows (k <= kProjSmall, the usual case): the
+// projection of each frame is formed on the fly in the final pass from the k
+// reduced coordinates, so no per-frame projection array is held, and the row
+// stays in registers in its input precision (widened exactly where used).
+// Same operations in the same order as project_rows, so the same results, with
+// about half the registers (more resident warps for this latency-bound pass).
+template <typename IN, int MAXF>
+__global__ void __launch_bounds__(128)
+    project_rows_one(const IN* __restrict__ x, IN* __restrict__ out, double* __restrict__ power, size_t rows,
+                     int nt, const double2* __restrict__ vec, int k, int mode, double inv_nt) {
+  const int lane = threadIdx.x & 31;
+  const size_t row = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32;
+  if (row >= rows) return;
+  IN xv[MAXF];
+#pragma unroll
+  for (int f = 0; f < MAXF; ++f) {
+    const int t = lane + 32 * f;
+    xv[f] = t < nt ? x[row * nt + t] : IN{};
+  }
+  double2 y[kProjSmall];
+  double retained = 0.0;
+#pragma unroll
+  for (int c = 0; c < kProjSmall; ++c) {
+    double yr = 0.0, yi = 0.0;
+    if (c < k) {  // k is uniform over the warp
+#pragma unroll
+      for (int f = 0; f < MAXF; ++f) {
+        const int t = lane + 32 * f;
+        if (t < nt) {
+          const double2 v = vec[t + size_t(c) * nt];
+          const double xr = double(xv[f].x), xi = double(xv[f].y);
+          yr = fma(xr, v.x, fma(-xi, v.y, yr));
+          yi = fma(xr, v.y, fma(xi, v.x, yi));
+        }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        yr += __shfl_xor_sync(0xffffffffu, yr, off);
+        yi += __shfl_xor_sync(0xffffffffu, yi, off);
+      }
+    }
+    y[c] = make_double2(yr, yi);
+    retained += yr * yr + yi * yi;
+  }
+  const bool subtract = mode & 1;
+  double pw = 0.0;
+  if (mode & 3) {
+#pragma unroll
+    for (int f = 0; f < MAXF; ++f) {
+      const int t = lane + 32 * f;
+      if (t < nt) {
+        double2 proj = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int c = 0; c < kProjSmall; ++c) {
+          if (c < k) {  // y * conj(v)
+            const double2 v = vec[t + size_t(c) * nt];
+            proj.x = fma(y[c].x, v.x, fma(y[c].y, v.y, proj.x));
+            proj.y = fma(y[c].y, v.x, fma(-y[c].x, v.y, proj.y));
+          }
+        }
+        const double2 r =
+            subtract ? make_double2(double(xv[f].x) - proj.x, double(xv[f].y) - proj.y) : proj;
+        pw += r.x * r.x + r.y * r.y;
+        if (mode & 2) {
+          if constexpr (sizeof(IN) == 8)
+            reinterpret_cast<float2*>(out)[row * nt + t] = make_float2(float(r.x), float(r.y));
+          else
+            reinterpret_cast<double2*>(out)[row * nt + t] = r;
+        }
+      }
+    }
+  }
+  if (power) {
+    if (subtract) {
+      for (int off = 16; off > 0; off >>= 1) pw += __shfl_xor_sync(0xffffffffu, pw, off);
+      if (lane == 0) power[row] = pw * inv_nt;
+    } else if (lane == 0) {
+      power[row] = retained * inv_nt;
+    }
+  }
+}
+
 }  // namespace clutter
 }  // namespace rcb

@@ -527,9 +527,14 @@ static cusolverDnHandle_t solver_handle() {
 template <typename IN, int MAXF>
 static void launch_project(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
                            size_t k, int mode) {
-  clutter::project_rows<IN, MAXF><<<blocks_for(rows * 32, 256), 256>>>(
-      static_cast<const IN*>(iq), static_cast<IN*>(out), power, rows, int(nt),
-      reinterpret_cast<const double2*>(vec), int(k), mode, 1.0 / double(nt));
+  if (k <= size_t(clutter::kProjSmall))
+    clutter::project_rows_one<IN, MAXF><<<blocks_for(rows * 32, 128), 128>>>(
+        static_cast<const IN*>(iq), static_cast<IN*>(out), power, rows, int(nt),
+        reinterpret_cast<const double2*>(vec), int(k), mode, 1.0 / double(nt));
+  else
+    clutter::project_rows<IN, MAXF><<<blocks_for(rows * 32, 256), 256>>>(
+        static_cast<const IN*>(iq), static_cast<IN*>(out), power, rows, int(nt),
+        reinterpret_cast<const double2*>(vec), int(k), mode, 1.0 / double(nt));
 }
 
 template <typename IN>
