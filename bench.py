@@ -9,8 +9,17 @@ aperture.  A step packs both apertures, beamforms OPW IQ with power, forms the
 temporal Gram matrix, eigendecomposes it and reduces the clutter-filtered
 power Doppler (rank_start = 3).
 
+Input: the seeded flow scene rendered on the GPU by the forward-model kernel
+(20,000 tissue speckle scatterers moving rigidly at 1 mm/s, 0 dB; 5,000 blood
+scatterers at -40 dB flowing at 10-30 mm/s through a 1 mm-radius tube; complex
+noise at -50 dB; PRF 500 Hz).
+
 Metric: OPW samples/s, one sample = voxel x receive channel x angle x frame
 over both apertures (2.362e12 per step), plus filtered-PD ms per ensemble.
+Accuracy: every form's filtered power against the plain form on the whole
+grid, and IQ / filtered power on a spread 2048-voxel sample against the
+float64 C oracle (the filtered power of the oracle IQ uses the float64 basis of
+the plain form's complex128 Gram).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -42,11 +51,15 @@ PITCH = 0.11e-3
 FS, FD, C = 20e6, 15e6, 1540.0
 T_START = 4e-6
 RANK_START = 3
-# DRAM bytes (read + write) per unit of the bf16x3 tensor-core DAS launch,
-# from one ncu capture on the central 64 x 128 x 64 block at 200 frames
-# (8192 work items): 45.09 GB read + 5.22 GB written for
-# 524,288 voxels x 256 ch x 11 ang x 200 frm.
-DAS_DRAM_BYTES_PER_UNIT = (45.085e9 + 5.220e9) / (524288 * 256 * 11 * 200)
+# DRAM bytes (read + write) of one full-size bf16x3 tensor-core DAS launch, from
+# an ncu capture of that launch (dram__bytes_read.sum + dram__bytes_write.sum).
+DAS_DRAM_BYTES_PER_LAUNCH = None
+DAS_DRAM_SOURCE = "not captured for this kernel revision"
+# DAS unit model: FP32-equivalent operations per interpolated sample -- the
+# lerp's two differences, two lerp FFMA and four FFMA of the complex rotate-
+# accumulate -- against 128 FP32 lanes per SM per clock.
+OPS_PER_UNIT = 8
+SAMPLE_VOXELS = 2048
 
 
 SUBGRID = None  # (nx, nz, ny) central block of the full grid, same spacing (profiling)
@@ -170,21 +183,58 @@ class _Null:
         return False
 
 
+def _scene(dev, seed: int):
+    """The flow scene at the workload's shapes (on the workload's grid, or its profiling block)."""
+    from rcabeam_b200 import scenes
+
+    scene = scenes.flow_scene(channels=NC, pitch=PITCH, samples=NS, angles=NA, frames=NT, grid_shape=GRID_SHAPE,
+                              t_start=T_START, seed=seed, device=dev)
+    scene.grid = workload()[2]
+    return scene
+
+
+def _sample_ids(nv: int) -> np.ndarray:
+    return np.unique(np.linspace(0, nv - 1, min(SAMPLE_VOXELS, nv)).round().astype(np.int64))
+
+
+def _scene_accuracy(scene, sample_ids, iq_sample: dict, powers: dict, basis_plain: np.ndarray, rank_start: int):
+    """IQ and filtered power of each form at the sample voxels against the float64 C oracle."""
+    from oracle import c_das
+    from rcabeam_b200.sim import scan_coords
+
+    f32 = lambda v: np.asarray(v, dtype=np.float32).astype(np.float64)  # noqa: E731
+    scan = scan_coords(scene.grid)[sample_ids].astype(np.float64)
+    geom = scene.geom
+    t0 = time.perf_counter()
+    want = c_das.opw_iq(scene.rc.cpu().numpy(), scene.cr.cpu().numpy(), scan, f32(geom.x_el), f32(geom.y_el),
+                        f32(scene.angles), f32([scene.t_start] * len(scene.angles)), float(np.float32(geom.c)),
+                        float(np.float32(geom.fs)), float(np.float32(geom.f_demod)), None)
+    oracle_s = time.perf_counter() - t0
+    nt = want.shape[1]
+    kept = basis_plain[:, rank_start:]
+    want_pd = np.sum(np.abs(want @ kept) ** 2, axis=1) / nt
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
+    out = {"sample_voxels": int(len(sample_ids)), "oracle_seconds": round(oracle_s, 1)}
+    for name, iq in iq_sample.items():
+        out[f"{name}_iq_rel_l2_vs_f64"] = rel(iq, want)
+        out[f"{name}_filtered_pd_rel_l2_vs_f64"] = rel(powers[name].cpu().numpy()[sample_ids], want_pd)
+    return out
+
+
 def run_b200(args, rank: int, world: int) -> dict | None:
     import torch
 
     from rcabeam_b200 import _lib, pipeline
-    from rcabeam_b200.sim import RCAGeometry
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    el, angles, grid = workload()
-    geom = RCAGeometry(el, el, c=C, fs=FS, f_demod=FD, fnumber=None)
-    gen = torch.Generator(device=dev).manual_seed(1234 + rank)
-    rc, cr = pipeline.synthetic_channels((NS, NC, NA, NT), generator=gen, device=dev)
+    scene = _scene(dev, seed=1234 + rank)
+    rc, cr, angles, grid, geom = scene.rc, scene.cr, scene.angles, scene.grid, scene.geom
     torch.cuda.synchronize()
     units = units_per_step()
-    results, powers = {}, {}
+    sample_ids = _sample_ids(int(np.prod(SUBGRID or GRID_SHAPE)))
+    results, powers, iq_sample = {}, {}, {}
+    basis_plain = None
     clock = None
     for name in ("chosen", "plain", "fp16_storage"):
         if name != "chosen" and args.only_chosen:
@@ -192,23 +242,28 @@ def run_b200(args, rank: int, world: int) -> dict | None:
         storage, precision = FORMS[name]
         plan = pipeline.FilteredOpw((NS, NC, NA, NT), angles, T_START, grid, geom, rank_start=RANK_START,
                                     precision=precision, iq_storage=storage)
-        steps = args.steps if name == "chosen" else max(1, min(args.steps, 2))
-        warm = args.warmup if name == "chosen" else 1
+        steps = args.steps if name == "chosen" else max(1, min(args.steps, 5))
+        warm = args.warmup if name == "chosen" else min(args.warmup, 2)
         sampler = ClockSampler(dev.index) if name == "chosen" else None
         elapsed, das_s, stages = _time_form(plan, rc, cr, steps, warm, world, sampler)
         if sampler is not None:
             clock = sampler.summary()
         powers[name] = plan.power.clone()
+        iq_sample[name] = plan.iq[torch.from_numpy(sample_ids).to(dev)].cpu().numpy()
+        if name == "plain":
+            nt = NT
+            vt = torch.view_as_complex(plan.gram.matrix.view(nt, nt, 2)).cpu().numpy()  # rows: ascending eigvecs
+            basis_plain = vt[::-1].T.copy()  # columns in descending order
         results[name] = {"ms_per_ensemble": round(elapsed / steps * 1e3, 3), "steps": steps,
                          "gsamples_per_s": round(units * world * steps / elapsed / 1e9, 3),
                          "das_ms": round(das_s * 1e3, 3), "stages_ms": stages, "iq_storage": storage,
                          "gram_precision": precision}
         if name == "chosen":
-            # End to end through the public pipeline: pinned host channels -> host filtered power.
+            # End to end through the public pipeline for a stream of ensembles: every step
+            # uploads its channels from pinned host memory (overlapping the previous step's
+            # reconstruction once that step has packed its channels) and reads its filtered
+            # power back.
             host_rc, host_cr = rc.cpu().pin_memory(), cr.cpu().pin_memory()
-            # End to end through the public API for a stream of ensembles: every step uploads its
-            # channels from pinned host memory (overlapping the previous step's reconstruction
-            # once that step has packed its channels) and reads its filtered power back.
             plan.run_host_sequence([(host_rc, host_cr)])
             e_steps = max(1, args.steps)
             outs = [torch.empty(plan.nv, dtype=torch.float64, pin_memory=True) for _ in range(e_steps)]
@@ -239,14 +294,21 @@ def run_b200(args, rank: int, world: int) -> dict | None:
         for name in ("chosen", "fp16_storage"):
             accuracy[f"{name}_vs_plain_filtered_pd_rel_l2"] = float(
                 torch.linalg.vector_norm(powers[name] - ref) / torch.linalg.vector_norm(ref))
+        if rank == 0 and not args.no_accuracy:
+            accuracy.update(_scene_accuracy(scene, sample_ids, iq_sample, powers, basis_plain, RANK_START))
     if rank != 0:
         return None
     ch = results["chosen"]
     pk = peaks()
     das_s = ch["das_ms"] / 1e3
-    # Tensor work of the dominant kernel: per (128-voxel tile, frame pass, aperture,
-    # channel, angle) step, two 64-voxel groups x 3 products of one
-    # M=128 x N=2*frames x K=16 MMA (sub-window splits excluded).
+    props = torch.cuda.get_device_properties(dev)
+    sms = props.multi_processor_count
+    mhz = (clock or {}).get("sm_mhz") or (clock or {}).get("sm_max_mhz") or 1965.0
+    units_per_s = units / das_s
+    fp32_peak = sms * 128 * mhz * 1e6  # FP32 lanes x clock (operations/s)
+    # Tensor work issued by the dominant kernel: per (128-voxel tile, frame pass, aperture,
+    # channel, angle) step, two 64-voxel groups x 3 products of one M=128 x N=2*frames x K=16
+    # MMA (sub-window splits excluded).
     tiles = (int(np.prod(SUBGRID or GRID_SHAPE)) + 127) // 128
     passes = (NT + 127) // 128
     full = 128 if NT > 128 else (NT + 7) // 8 * 8
@@ -263,27 +325,37 @@ def run_b200(args, rank: int, world: int) -> dict | None:
         "ms_per_step": ch["ms_per_ensemble"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 math on bf16x2-split c64 IQ (tcgen05 3-product DAS), 3xBF16 tcgen05 Gram with f64 flushes, "
                  "f64 eig/projection",
-        "data": "synthetic seeded channel IQ (complex Gaussian), full-size shapes", "config": CONFIG,
+        "data": "synthetic: seeded flow scene (tissue 0 dB at 1 mm/s, blood -40 dB at 10-30 mm/s in a 1 mm tube, "
+                "noise -50 dB) rendered by the forward-model kernel at the full-size shapes",
+        "config": {**CONFIG, "scene": scene.info["scene"], "scene_seed": scene.info["seed"]},
         "filtered_pd_ms_per_ensemble": {"chosen": ch["ms_per_ensemble"],
                                          **({"plain": results["plain"]["ms_per_ensemble"]} if "plain" in results else {})},
         "forms": results, "accuracy": accuracy, "e2e": e2e,
-        "roofline": {"bound": "tensor", "kernel": "opw_tc<bf16x3> (DAS)",
-                     "achieved": round(mma_flops / das_s / 1e12, 1), "peak": tensor_peak, "unit": "TFLOP/s",
-                     "frac": round(mma_flops / das_s / 1e12 / tensor_peak, 4), "peak_source": peak_source,
-                     "traffic": round(DAS_DRAM_BYTES_PER_UNIT * units),
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one opw_tc launch on the "
-                                       "central 64x128x64 block (200 frames), scaled by units "
-                                       "(profiles/opw_tc_bf16x3_central_blocks_200frames_ncu.md)",
-                     "das_ms": ch["das_ms"],
-                     "note": "dense tcgen05 MMA flops issued per launch (2 groups x 3 products x M128 x N(2 x pass "
-                             f"frames {pass_frames}) x K16 per 128-voxel tile step) vs "
-                             f"sustained bf16 peak (of {peak_source}); compulsory HBM bytes "
-                             f"{das_bytes / 1e9:.2f} GB per launch -> {das_bytes / das_s / 1e9:.1f} GB/s"},
+        "roofline": {
+            "bound": "tensor", "kernel": "opw_tc<bf16x3> (DAS on tcgen05)",
+            "achieved": round(OPS_PER_UNIT * units_per_s / 1e12, 2), "peak": round(fp32_peak / 1e12, 2),
+            "unit": "TFLOP/s", "frac": round(OPS_PER_UNIT * units_per_s / fp32_peak, 4),
+            "units_per_s": round(units_per_s, -6), "das_ms": ch["das_ms"],
+            "model": f"FP32-issue-equivalent ceiling: {OPS_PER_UNIT} FP32 operations per interpolated sample "
+                     f"(2 lerp differences, 2 lerp FFMA, 4 FFMA complex rotate-accumulate) x units/s, against "
+                     f"{sms} SMs x 128 FP32 lanes x the median SM clock under load ({mhz:g} MHz); "
+                     "frac = units/s / (SMs x 16 x clock)",
+            "smem_gather_model": "16 B of shared-memory gathers per unit (2 float32 complex taps) at 128 B/clk/SM "
+                                 "bounds a per-sample gather kernel (the SIMT float32 path); the tensor-core kernel "
+                                 "stages each 16-row window once per 128-voxel tile and reads it through the MMA, "
+                                 "so it does not bound this kernel",
+            "issued_mma_tflops": round(mma_flops / das_s / 1e12, 1),
+            "issued_mma_frac_of_bf16": round(mma_flops / das_s / 1e12 / tensor_peak, 4),
+            "bf16_peak_tflops": tensor_peak, "peak_source": peak_source,
+            "traffic": DAS_DRAM_BYTES_PER_LAUNCH, "traffic_source": DAS_DRAM_SOURCE,
+            "compulsory_hbm_bytes": das_bytes,
+            "note": f"compulsory HBM bytes {das_bytes / 1e9:.2f} GB per launch -> {das_bytes / das_s / 1e9:.1f} GB/s: "
+                    "the DAS cannot be HBM-bound on algorithmic bytes"},
         "clocks": clock,
         "gpu_launches": launches * args.steps,
     }
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args, reference_arm=False)
+        line["cpu_baseline"] = cpu_baseline(args, voxels_per_core=args.cpu_voxels)
     return line
 
 
@@ -590,7 +662,7 @@ def run_differentiation(args) -> dict:
 
 # ------------------------------------------------------- CPU (oracle) arms --
 def _oracle_sample(seed: int, voxels: int):
-    """A bounded slice of the workload for the float64 CPU oracle: the first voxels of the grid."""
+    """A bounded slice of the workload for the float64 CPU oracle: voxels spread over the grid."""
     from oracle import das
 
     el, angles, grid = workload()
@@ -598,8 +670,9 @@ def _oracle_sample(seed: int, voxels: int):
     shape = (NS, NC, NA, NT)
     rc = (rng.standard_normal(shape, dtype=np.float32) + 1j * rng.standard_normal(shape, dtype=np.float32))
     cr = (rng.standard_normal(shape, dtype=np.float32) + 1j * rng.standard_normal(shape, dtype=np.float32))
-    scan = das.scan_coords(grid)[:voxels].astype(np.float64)
-    return rc.astype(np.complex64), cr.astype(np.complex64), scan, el, angles
+    scan = das.scan_coords(grid).astype(np.float64)
+    ids = np.unique(np.linspace(0, len(scan) - 1, voxels).round().astype(np.int64))
+    return rc.astype(np.complex64), cr.astype(np.complex64), scan[ids], el, angles
 
 
 _SHARED = {}
@@ -619,22 +692,27 @@ def _attach(names, shape, el, angles):
 def _oracle_chunk(scan):
     from oracle import das
 
-    iq = das.opw_iq(_SHARED["rc"], _SHARED["cr"], scan, _SHARED["el"], _SHARED["el"], _SHARED["angles"], T_START,
-                    C, FS, FD, None)
-    return das.power_doppler(iq)
+    return das.opw_iq(_SHARED["rc"], _SHARED["cr"], scan, _SHARED["el"], _SHARED["el"], _SHARED["angles"], T_START,
+                      C, FS, FD, None)
 
 
-def cpu_baseline(args, reference_arm: bool) -> dict:
-    """Time the float64 oracle port of the reference NumPy path on a bounded voxel sample.
+def cpu_baseline(args, voxels_per_core: int) -> dict:
+    """Time the float64 NumPy restatement of the reference's CPU path on a bounded voxel sample, on
+    every host core: DAS + OPW of the sample (reference sim._delay_numpy / opw.py), then the Gram
+    clutter filter over the sample's rows and the filtered power (clutter.py:74-109, power.py).
 
-    The channels live in shared memory that every worker maps; the pool is
-    started before the timed region, which covers only the DAS + OPW + PD work."""
+    The channels live in shared memory that every worker maps; the spawn pool is started
+    before the timed region.  The sample is the same fraction of every stage's work (all
+    stages are linear in the voxel count), so units / seconds is the path's rate."""
     import multiprocessing as mp
     from multiprocessing import shared_memory
 
-    cores = (os.cpu_count() or 1) if reference_arm else 1
-    voxels = args.cpu_voxels * cores
+    from oracle import clutter as oc
+
+    cores = os.cpu_count() or 1
+    voxels = voxels_per_core * cores
     rc, cr, scan, el, angles = _oracle_sample(7, voxels)
+    voxels = len(scan)
     blocks = {}
     try:
         for key, arr in (("rc", rc), ("cr", cr)):
@@ -642,41 +720,34 @@ def cpu_baseline(args, reference_arm: bool) -> dict:
             np.ndarray(arr.shape, dtype=np.complex64, buffer=blocks[key].buf)[...] = arr
         names = {k: b.name for k, b in blocks.items()}
         chunks = np.array_split(scan, cores)
-        if cores > 1:
-            with mp.get_context("spawn").Pool(cores, initializer=_attach,
-                                              initargs=(names, rc.shape, el, angles)) as pool:
-                pool.map(len, [[0]] * cores)  # workers started and attached
-                begin = time.perf_counter()
-                pool.map(_oracle_chunk, chunks)
-                seconds = time.perf_counter() - begin
-        else:
-            _attach(names, rc.shape, el, angles)
+        with mp.get_context("spawn").Pool(cores, initializer=_attach, initargs=(names, rc.shape, el, angles)) as pool:
+            pool.map(len, [[0]] * cores)  # workers started and attached
             begin = time.perf_counter()
-            _oracle_chunk(scan)
+            iq = np.concatenate(pool.map(_oracle_chunk, chunks))
+            _, basis = oc.temporal_basis(iq, method="gram")
+            oc.filtered_power(iq, basis, RANK_START)
             seconds = time.perf_counter() - begin
     finally:
-        for key in ("rc", "cr"):
-            _SHARED.pop(key, None)
-            b = _SHARED.pop(key + "_block", None)
-            if b is not None:
-                b.close()
         for b in blocks.values():
             b.close()
             b.unlink()
     units = voxels * 2 * NC * NA * NT
     return {"value": round(units / seconds / 1e9, 5), "unit": "Gsamples/s", "cores": cores, "kind": "port",
-            "sample": f"{voxels} voxels x 256 ch x 11 ang x 200 frm of the workload (DAS + OPW + PD, float64 NumPy "
-                      f"restatement of reference sim._delay_numpy), {seconds:.1f} s"}
+            "sample": f"{voxels} voxels spread over the grid x 256 ch x 11 ang x 200 frm of the workload: DAS + OPW "
+                      "(float64 NumPy restatement of reference sim._delay_numpy), Gram clutter filter over the "
+                      f"sample rows and filtered PD (restatement of clutter.py:74-109), {seconds:.1f} s"}
 
 
 def run_reference(args, rank: int, world: int) -> dict | None:
+    """The reference arm: the float64 NumPy restatement of the reference's CPU path, one bounded
+    sample per step on all host cores (rank 0 only)."""
     if rank != 0:
         return None
     vals = []
     for _ in range(args.warmup):
-        cpu_baseline(args, reference_arm=True)
+        cpu_baseline(args, voxels_per_core=args.reference_voxels)
     for _ in range(args.steps):
-        vals.append(cpu_baseline(args, reference_arm=True))
+        vals.append(cpu_baseline(args, voxels_per_core=args.reference_voxels))
     value = statistics.median(v["value"] for v in vals)
     base = dict(vals[-1])
     base["value"] = value
@@ -695,9 +766,12 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--cpu-voxels", type=int, default=1536,
-                    help="oracle voxels per core for the CPU baseline (~15 s of one core)")
+    ap.add_argument("--cpu-voxels", type=int, default=768,
+                    help="oracle voxels per core for the CPU baseline of the B200 line (~10 s)")
+    ap.add_argument("--reference-voxels", type=int, default=192,
+                    help="oracle voxels per core per step of the reference arm (~3 s per step)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the float64 oracle sample (profiling runs)")
     ap.add_argument("--only-chosen", action="store_true", help="time only the chosen form (profiling runs)")
     ap.add_argument("--grid", type=int, nargs=3, default=None, metavar=("NX", "NZ", "NY"),
                     help="reduced grid for profiling runs (the reported workload is the default)")

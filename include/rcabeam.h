@@ -216,9 +216,11 @@ rcabeam_status rcabeam_project_device(const void* iq, void* out, double* power, 
 rcabeam_status rcabeam_ensemble_workspace_bytes(size_t nv, size_t nc, size_t na, size_t* bytes);
 
 /* Same computation as rcabeam_ensemble_device (methods 0, 1, 2, 3 and 5), for
- * callers that cannot allocate device memory: it takes no geometry workspace
- * and keeps its scratch in a fixed 8 MiB array inside the library, so the call
- * itself never allocates.  No counterpart in the reference interface.
+ * callers that cannot allocate device memory -- acquisition loops whose memory
+ * budget is fixed up front, plugins whose host owns the device allocator: it
+ * takes no geometry workspace and keeps its scratch in a fixed 8 MiB array
+ * inside the library, so the call itself never allocates.  No counterpart in
+ * the reference interface.
  * Limits: nv <= 262144 voxels per call (RCABEAM_ERROR_ARGUMENT beyond, and for
  * method 4).  All calls on a device share the scratch: calls that overlap on
  * the GPU (other streams or threads) race.  The first call on each device
@@ -304,6 +306,22 @@ rcabeam_status rcabeam_batch_prepare(size_t n, const rcabeam_batch_ensemble* lis
 rcabeam_status rcabeam_batch_run_device(size_t n, const rcabeam_batch_ensemble* list, void* table,
                                         size_t table_bytes, unsigned long long* times, int ctas_per_sm,
                                         void* stream);
+
+/* Scene synthesis (extension; test and benchmark input, no counterpart in the
+ * reference C interface).  Writes out = channel IQ (ns, nc, na, nt) complex64
+ * of one aperture (config 0 = RC receiving on x elements, 1 = CR on y) for n
+ * moving point scatterers, the Gaussian-pulse model of the reference's
+ * simulate_point (src/rcabeam/sim.py:131-189):
+ *   sum_k amp_k exp(-((t - tau)/sigma_t)^2) exp(-j 2 pi fd tau),
+ * t = starts[a] + i / fs, evaluated where |t - tau| <= half_width.
+ * scatterers: n x 11 floats (ox, oz, oy, dx, dz, dy, s0, speed, period,
+ * amp_re, amp_im); at frame f (time f / prf) a scatterer sits at
+ * o + d * s with s = s0 + speed * f / prf, wrapped into [0, period) when
+ * period > 0.  Every element of out is written. */
+rcabeam_status rcabeam_simulate_scene_device(const float* scatterers, size_t n, const float* elements,
+                                             const float* angles, const float* starts, void* out, size_t ns,
+                                             size_t nc, size_t na, size_t nt, int config, double prf, double c,
+                                             double fs, double fd, double sigma_t, double half_width);
 
 /* Workspace bytes of rcabeam_voxel_order_device for nv voxels (128 <= nv < 2^31). */
 rcabeam_status rcabeam_voxel_order_workspace_bytes(size_t nv, size_t* bytes);

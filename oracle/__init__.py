@@ -10,7 +10,11 @@ of sdiebolt/rcabeam for the OPW path:
                   DMAS-CCF-ACF (dmas.py:32-85), evaluated per frame;
 * ``clutter``  -- the global temporal SVD clutter filter
                   (src/rcabeam/clutter.py:10-109) in complex128;
-* ``adjoint``  -- the float64 adjoint of the DAS forward model.
+* ``adjoint``  -- the float64 adjoint of the DAS forward model;
+* ``c_das``    -- the same float64 DAS in C (``das_c.c``, threaded), for grids
+                  where the NumPy restatement is too slow;
+* ``scene``    -- the float64 forward model of moving point-scatterer scenes
+                  (the reference's simulate_point pulse, src/rcabeam/sim.py:131-189).
 
 Only the test suite, ``__graft_entry__.smoke()`` and the ``cpu_baseline`` /
 ``--impl reference`` legs of ``bench.py`` may import it, and only as the

@@ -11,11 +11,12 @@ Nothing is copied into the repository: the output goes to ``oracle/_ref/``,
 which git ignores.  When the reference sources are absent (on a machine that
 only runs the prebuilt files) the recipe leaves an existing build untouched.
 
-    python oracle/build_ref.py [reference_root]
+    python oracle/build_ref.py <reference_root>     (or RCABEAM_REFERENCE=<reference_root>)
 """
 
 from __future__ import annotations
 
+import os
 import shutil
 import subprocess
 import sys
@@ -23,11 +24,10 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref" / "librcabeam_ref.so"
-DEFAULT_ROOT = Path("/root/reference")
 SOURCES = ("src/rcabeam/core.cu", "src/rcabeam/ensemble.cu")
 
 
-def build(reference_root: Path = DEFAULT_ROOT, verbose: bool = False) -> Path | None:
+def build(reference_root: Path, verbose: bool = False) -> Path | None:
     sources = [reference_root / s for s in SOURCES]
     header = reference_root / "include" / "rcabeam.h"
     if not header.exists() or not all(s.exists() for s in sources):
@@ -50,5 +50,7 @@ def build(reference_root: Path = DEFAULT_ROOT, verbose: bool = False) -> Path | 
 
 
 if __name__ == "__main__":
-    root = Path(sys.argv[1]) if len(sys.argv) > 1 else DEFAULT_ROOT
-    print(build(root, verbose=True))
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RCABEAM_REFERENCE")
+    if not root:
+        sys.exit("usage: build_ref.py <reference checkout> (or set RCABEAM_REFERENCE)")
+    print(build(Path(root), verbose=True))

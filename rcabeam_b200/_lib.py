@@ -51,6 +51,7 @@ SIGNATURES: dict[str, list] = {
     "rcabeam_batch_table_bytes": [Z, P, ctypes.POINTER(c_size_t)],
     "rcabeam_batch_prepare": [Z, P, P, Z],
     "rcabeam_batch_run_device": [Z, P, P, Z, P, I, P],
+    "rcabeam_simulate_scene_device": [P, Z, P, P, P, P, Z, Z, Z, Z, I, D, D, D, D, D, D],
     "rcabeam_voxel_order_workspace_bytes": [Z, ctypes.POINTER(c_size_t)],
     "rcabeam_voxel_order_device": [P, Z, P, P, Z],
     "rcabeam_device_error": [ctypes.POINTER(c_int)],

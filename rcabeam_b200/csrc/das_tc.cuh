@@ -112,6 +112,7 @@ struct Args {
   int ncols;       // 2 * frames
   int nbox;        // TMA boxes per plane of a full pass (the stage layout)
   int ntiles;
+  int walk_fixed;  // 1: every item walks the channel slots from slot 0 (run-to-run identical sums)
   int* err;
 };
 
@@ -488,7 +489,7 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
       // different slabs together touch more sample windows than L2 holds.
       // The walk order only changes the order of the float32 sums.
       if (warp == 0 && lane == 0)
-        *walk_start = int((*reinterpret_cast<volatile unsigned long long*>(p.slot_clock) / gridDim.x) %
+        *walk_start = p.walk_fixed ? 0 : int((*reinterpret_cast<volatile unsigned long long*>(p.slot_clock) / gridDim.x) %
                           (2ull * unsigned(p.nc)));
       builders_sync();
       int steps = 0;

@@ -7,7 +7,9 @@
 #include <cmath>
 #include <cstdint>
 #include <cub/device/device_radix_sort.cuh>
+#include <cstdlib>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include <cusolverDn.h>
@@ -19,8 +21,10 @@
 #include "das_generic.cuh"
 #include "das_staged.cuh"
 #include "das_tc.cuh"
+#include "das_tm.cuh"
 #include "gram_tc.cuh"
 #include "pack.cuh"
+#include "scene.cuh"
 
 namespace rcb {
 
@@ -325,8 +329,65 @@ static float2* tc_partials_address() {
   return addresses[dev];
 }
 
+// Frames of the full passes of the TMEM-coefficient kernel (multiple of 8, <= 104).
+static size_t tm_full_frames(size_t nt) {
+  return nt > size_t(tm::kMaxFrames) ? size_t(tm::kMaxFrames) : (nt + 7) / 8 * 8;
+}
+
+// Tensor-core OPW with the coefficients in tensor memory (das_tm.cuh).
+template <bool BF16X3>
+static rcabeam_status run_tm(tc::Args a) {
+  const size_t nt = size_t(a.nt);
+  a.chunks = int((nt + tm::kMaxFrames - 1) / tm::kMaxFrames);
+  const int frames = int(tm_full_frames(nt));
+  a.frames = frames;
+  a.last_frames = int((nt - size_t(frames) * size_t(a.chunks - 1) + 7) / 8 * 8);
+  a.ncols = 2 * frames;
+  a.nbox = (a.ncols + tc::kBoxCols - 1) / tc::kBoxCols;
+  a.ntiles = int((size_t(a.nv) + tc::kVox - 1) / tc::kVox);
+  const size_t smem = tm::Layout<BF16X3>::bytes(a.nbox, a.na) + 1024;
+  if (smem > 227 * 1024) return RCABEAM_ERROR_ARGUMENT;
+  CUtensorMap mh[2], ml[2];
+  const size_t slabs = size_t(a.nc) * a.na;
+  for (int i = 0; i < 2; ++i) {
+    if (!make_plane_map(&mh[i], a.x_hi[i], nt, size_t(a.ns), slabs)) return RCABEAM_ERROR_CUDA;
+    if (BF16X3) {
+      if (!make_plane_map(&ml[i], a.x_lo[i], nt, size_t(a.ns), slabs)) return RCABEAM_ERROR_CUDA;
+    } else {
+      ml[i] = mh[i];
+    }
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  auto kern = tm::opw_tm<BF16X3>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+    return RCABEAM_ERROR_CUDA;
+  a.partial = tc_partials_address();
+  a.slot_clock = tc_slot_clock_address();
+  if (!a.partial || !a.slot_clock) return RCABEAM_ERROR_CUDA;
+  const int items = a.ntiles * a.chunks;
+  const unsigned grid = unsigned(std::min(std::min(items, sms), tc::kMaxCtas));
+  kern<<<grid, tm::kThreads, smem>>>(mh[0], mh[1], ml[0], ml[1], a);
+  return launch_status();
+}
+
+// Which tensor-core OPW kernel runs: the TMEM-coefficient kernel unless
+// RCABEAM_DAS_KERNEL=smem selects the shared-memory-coefficient one (a/b timing).
+static bool use_tm_kernel() {
+  const char* v = std::getenv("RCABEAM_DAS_KERNEL");
+  return !(v && std::string(v) == "smem");
+}
+
+static bool deterministic_walk() {
+  const char* v = std::getenv("RCABEAM_DETERMINISTIC");
+  return v && v[0] == '1';
+}
+
 template <bool BF16X3>
 static rcabeam_status run_tc(tc::Args a) {
+  a.walk_fixed = deterministic_walk() ? 1 : 0;
+  if (use_tm_kernel()) return run_tm<BF16X3>(a);
   const size_t nt = size_t(a.nt);
   // The deepest ring (one builder warp per stage) that fits shared memory.
   int stages = tc::kDeepStages;
@@ -537,9 +598,44 @@ static void launch_project(const void* iq, void* out, double* power, size_t rows
         reinterpret_cast<const double2*>(vec), int(k), mode, 1.0 / double(nt));
 }
 
+// Streamed projection (complex64 rows, k <= 4, even nt <= 512, 16-byte aligned
+// rows): one CTA per SM, G lanes per row.  False when the form does not apply.
+template <int G>
+static bool launch_project_pipe(const void* iq, void* out, double* power, size_t rows, size_t nt,
+                                const double* vec, size_t k, int mode) {
+  using S = clutter::PipeShape<G>;
+  auto kern = clutter::project_rows_pipe<G>;
+  const size_t smem = S::smem_bytes(int(nt));
+  if (smem > 227 * 1024 ||
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+    return false;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t blocks = (rows + S::kRows - 1) / S::kRows;
+  const unsigned grid = unsigned(std::min<size_t>(blocks, size_t(sms)));
+  kern<<<grid, S::kThreads, smem>>>(static_cast<const float2*>(iq), static_cast<float2*>(out), power, rows, int(nt),
+                                    reinterpret_cast<const double2*>(vec), int(k), mode, 1.0 / double(nt),
+                                    device_error_ptr());
+  return true;
+}
+
+static bool project_pipe(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
+                         size_t k, int mode) {
+  if (k > size_t(clutter::kProjSmall) || nt % 2 || nt > 512 || reinterpret_cast<uintptr_t>(iq) % 16 != 0 ||
+      rows > (size_t(1) << 40))
+    return false;
+  if (nt <= 128) return launch_project_pipe<4>(iq, out, power, rows, nt, vec, k, mode);
+  if (nt <= 256) return launch_project_pipe<8>(iq, out, power, rows, nt, vec, k, mode);
+  return launch_project_pipe<16>(iq, out, power, rows, nt, vec, k, mode);
+}
+
 template <typename IN>
 static void project_dispatch(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
                              size_t k, int mode) {
+  if constexpr (sizeof(IN) == 8) {
+    if (project_pipe(iq, out, power, rows, nt, vec, k, mode)) return;
+  }
   size_t f = (nt + 31) / 32;
   if (f <= 1) launch_project<IN, 1>(iq, out, power, rows, nt, vec, k, mode);
   else if (f <= 2) launch_project<IN, 2>(iq, out, power, rows, nt, vec, k, mode);
@@ -549,14 +645,15 @@ static void project_dispatch(const void* iq, void* out, double* power, size_t ro
 }
 
 // ---------------------------------------------- no-allocation entry point --
-// Some callers cannot call cudaMalloc at all: code running inside a CUDA graph
-// they are recording, real-time acquisition loops whose memory budget is fixed
-// up front, or hosts whose allocator is owned by another runtime.  For them
-// rcabeam_ensemble_static_device keeps its scratch (the voxel traversal-order
-// sort: keys, values, bounding box and radix-sort temporaries) in this
-// file-scope device array instead of a caller-provided workspace.  Every GPU
-// that loads the library holds the array until the process exits, and every
-// call on a device shares it.
+// Some callers cannot call cudaMalloc at all: real-time acquisition loops whose
+// device memory budget is fixed when the scanner starts (an allocation can
+// synchronize the device and stall the loop for an unbounded time), and
+// plugins inside host applications whose device memory belongs to another
+// runtime's allocator.  For them rcabeam_ensemble_static_device keeps its
+// scratch (the voxel traversal-order sort: keys, values, bounding box and
+// radix-sort temporaries) in this file-scope device array instead of a
+// caller-provided workspace.  Every GPU that loads the library holds the array
+// until the process exits, and every call on a device shares it.
 constexpr size_t kStaticMaxVoxels = size_t(1) << 18;       // 262144 voxels per call
 constexpr size_t kStaticScratchBytes = size_t(8) << 20;    // 8 MiB per device
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
@@ -592,6 +689,10 @@ static rcabeam_status ensemble_static(const void* rc, const void* cr, const floa
     return RCABEAM_ERROR_ARGUMENT;
   void* scratch = static_scratch_address();
   if (!scratch) return RCABEAM_ERROR_CUDA;
+  // The sort's scratch for the largest accepted call must fit the array (the
+  // radix-sort temporaries depend on the CUB version): checked once, on the host.
+  static const bool fits = order_bytes(kStaticMaxVoxels, nullptr) <= kStaticScratchBytes;
+  if (!fits) return RCABEAM_ERROR_CUDA;
   if (cudaMemsetAsync(pd, 0, 2 * nv * sizeof(float), 0) != cudaSuccess) return RCABEAM_ERROR_CUDA;
   das::Args a{};
   a.rc = rc;
@@ -620,7 +721,9 @@ static rcabeam_status ensemble_static(const void* rc, const void* cr, const floa
     return launch_status();
   }
   // The sort rewrites keys, values and the bounding box (cleared inside) on every call.
+  // Calls too small to need an order run in identity order; a failed sort is an error.
   a.order = voxel_order(scan, nv, scratch, kStaticScratchBytes);
+  if (!a.order && order_bytes(nv, nullptr)) return RCABEAM_ERROR_CUDA;
   if (method == 3) return run_dmas_staged(a, (nv + das::kTileVoxels - 1) / das::kTileVoxels);
   const size_t ntiles = (nv + das::kTileVoxels - 1) / das::kTileVoxels;
   rcabeam_status st = method == 0   ? run_staged<false, das::kOpw>(a, ntiles)
@@ -1313,6 +1416,46 @@ rcabeam_status rcabeam_batch_run_device(size_t n, const rcabeam_batch_ensemble* 
   const unsigned grid = unsigned(total < want ? total : want);
   kern<<<grid, das::kThreads, batch::Smem::kBytes, st>>>(batch_queue(table, n, L, total, times));
   return cudaGetLastError() == cudaSuccess ? RCABEAM_SUCCESS : RCABEAM_ERROR_CUDA;
+}
+
+rcabeam_status rcabeam_simulate_scene_device(const float* scatterers, size_t n, const float* elements,
+                                             const float* angles, const float* starts, void* out, size_t ns,
+                                             size_t nc, size_t na, size_t nt, int config, double prf, double c,
+                                             double fs, double fd, double sigma_t, double half_width) {
+  if (!scatterers || !elements || !angles || !starts || !out || !n || ns < 2 || !nc || !na || !nt ||
+      (config != 0 && config != 1) || !(prf > 0) || !(c > 0) || !(fs > 0) || !std::isfinite(fd) ||
+      !(sigma_t > 0) || !(half_width > 0) || ns > 16384 || nc * na > 65535 || nt > INT32_MAX ||
+      n > SIZE_MAX / scene::kFields)
+    return RCABEAM_ERROR_ARGUMENT;
+  // Frame chunk: the (samples x chunk) complex64 slab stays within 96 KB (two CTAs per SM).
+  size_t chunk = (96 * 1024) / (ns * sizeof(float2));
+  if (chunk < 1) chunk = 1;
+  if (chunk > nt) chunk = nt;
+  const size_t smem = ns * chunk * sizeof(float2);
+  if (cudaFuncSetAttribute(scene::simulate, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+    return RCABEAM_ERROR_CUDA;
+  scene::Args a{};
+  a.scatterers = scatterers;
+  a.n = n;
+  a.elements = elements;
+  a.angles = angles;
+  a.starts = starts;
+  a.out = static_cast<float2*>(out);
+  a.ns = int(ns);
+  a.nc = int(nc);
+  a.na = int(na);
+  a.nt = int(nt);
+  a.chunk = int(chunk);
+  a.config = config;
+  a.prf = prf;
+  a.c = c;
+  a.fs = fs;
+  a.fd = fd;
+  a.sigma = sigma_t;
+  a.half_width = half_width;
+  const dim3 grid(unsigned(nc * na), unsigned((nt + chunk - 1) / chunk));
+  scene::simulate<<<grid, scene::kThreads, smem>>>(a);
+  return launch_status();
 }
 
 rcabeam_status rcabeam_voxel_order_workspace_bytes(size_t nv, size_t* bytes) {

@@ -1,7 +1,8 @@
 """Frame-batched RCA reconstruction: the public entry points of ``rcabeam.ensemble``.
 
-Same signatures, validation and error messages as the reference
-(src/rcabeam/ensemble.py:52-287); the work runs through the C ABI on the GPU.
+Same signatures and argument contract as the reference
+(src/rcabeam/ensemble.py:52-287), checked by the shared validator
+``rcabeam_b200._inputs``; the work runs through the C ABI on the GPU.
 Host NumPy arrays are uploaded and results downloaded, as in the reference.
 """
 
@@ -12,12 +13,11 @@ from typing import Literal, TypedDict
 import numpy as np
 from numpy.typing import NDArray
 
-from rcabeam_b200 import _cuda_impl
-from rcabeam_b200.sim import RCAGeometry, scan_coords
+from rcabeam_b200 import _cuda_impl, _inputs
+from rcabeam_b200.sim import RCAGeometry
 
 Method = Literal["opw", "xdoppler", "rc_fmas", "dmas", "st_sw"]
 IQStorage = Literal["float32", "float16", "bf16x2"]
-_METHODS = {"opw": 0, "xdoppler": 1, "rc_fmas": 2, "dmas": 3, "st_sw": 4, "apertures": 5}
 
 
 class EnsembleTiming(TypedDict):
@@ -51,63 +51,35 @@ def opw_voxel_order(shape: tuple[int, int, int]) -> NDArray[np.intp]:
 
 def _run(rc, cr, angles, t_start, grid, geom: RCAGeometry, method, k: int, return_signal: bool,
          timings: EnsembleTiming | None, iq_storage: IQStorage):
-    """Validate ensemble inputs and execute the frame-batched CUDA path (reference ensemble.py:52-130)."""
-    if method not in _METHODS or (method == "apertures" and not return_signal):
-        raise ValueError(f"Unknown method: {method}")
-    if iq_storage not in ("float32", "float16", "bf16x2") or (iq_storage != "float32" and method != "opw"):
-        raise ValueError("IQ storage must be float32, or float16 / bf16x2 for OPW only")
+    """Check the inputs once (``_inputs.acquisition``), reconstruct on the GPU, shape the outputs.
+
+    The argument contract is the reference's (ensemble.py:52-130): same accepted inputs, the
+    contract's message substrings.  Power comes back in canonical voxel order (the kernels
+    write canonical positions from their own traversal), so no host un-permutation is needed.
+    """
     rc, cr = np.asarray(rc), np.asarray(cr)
-    if rc.ndim != 4 or cr.shape != rc.shape or any(n == 0 for n in rc.shape) or rc.shape[0] < 2:
-        raise ValueError("RC/CR must have matching nonempty (samples, channels, angles, frames) shapes")
-    if len(angles) != rc.shape[2] or len(geom.x_el) != rc.shape[1] or len(geom.y_el) != rc.shape[1]:
-        raise ValueError("Geometry must match the channel/angle dimensions")
-    if any(np.ndim(axis) != 1 or not len(axis) or not np.isfinite(axis).all() for axis in grid):
-        raise ValueError("Grid axes must be nonempty finite coordinate vectors")
-    if not np.isfinite([geom.c, geom.fs, geom.f_demod]).all() or geom.c <= 0 or geom.fs <= 0:
-        raise ValueError("Sound speed and sampling frequency must be finite and positive")
-    if geom.fnumber is not None and (not np.isfinite(geom.fnumber) or geom.fnumber <= 0):
-        raise ValueError("F-number must be positive or None")
-    if method == "st_sw" and (k < 2 or k > 4 or len(angles) < k):
-        raise ValueError("St-SW requires 2 <= k <= 4 and at least k angles")
-    starts = np.ascontiguousarray(np.broadcast_to(np.asarray(t_start, dtype=np.float32), (len(angles),)))
-    if not all(np.isfinite(a).all() for a in (angles, starts, geom.x_el, geom.y_el)):
-        raise ValueError("Geometry and sample starts must be finite")
-    scan = scan_coords(grid)
-    nv, nt = len(scan), rc.shape[-1]
-    shape = (len(grid[0]), len(grid[1]), len(grid[2]))
-    pd = np.empty((nv, 2), dtype=np.float32)
+    code = _inputs.method_code(method, iq_storage, wants_signal=return_signal)
+    acq = _inputs.acquisition(_inputs.channel_pair_shape(rc, cr), angles, t_start, grid, geom)
+    _inputs.check_subsets(method, k, acq.channel_shape[2])
+    nv, nt = acq.voxels, acq.channel_shape[3]
     planes = 2 if method == "apertures" else 1
+    pd = np.empty((nv, 2), dtype=np.float32)
     signal = np.empty((nv * planes if return_signal else 0, nt), dtype=np.complex64)
     weights = np.empty(nv if method == "st_sw" else 0, dtype=np.float32)
-    raw_upload_seconds = _cuda_impl.ensemble_from_channels(
-        np.ascontiguousarray(rc, dtype=np.complex64),
-        np.ascontiguousarray(cr, dtype=np.complex64),
-        scan,
-        np.ascontiguousarray(geom.x_el, dtype=np.float32),
-        np.ascontiguousarray(geom.y_el, dtype=np.float32),
-        np.ascontiguousarray(angles, dtype=np.float32),
-        starts,
-        pd,
-        signal,
-        weights,
-        float(geom.c),
-        float(geom.fs),
-        float(geom.f_demod),
-        -1.0 if geom.fnumber is None else float(geom.fnumber),
-        _METHODS[method],
-        k,
-        iq_storage,
-    )
+    upload_s = _cuda_impl.ensemble_from_channels(
+        np.ascontiguousarray(rc, dtype=np.complex64), np.ascontiguousarray(cr, dtype=np.complex64), acq.scan,
+        acq.x_el, acq.y_el, acq.angles, acq.starts, pd, signal, weights, *acq.constants, code, k, iq_storage)
     if timings is not None:
-        timings["raw_upload_seconds"] = raw_upload_seconds
+        timings["raw_upload_seconds"] = upload_s
+    power = pd[:, 0]
     if method == "st_sw":
-        # Raw weights normalized by the full-volume peak (reference ensemble.py:127-129).
+        # Raw weights normalized by the whole volume's peak (reference ensemble.py:127-129).
         peak = weights.max()
-        pd[:, 0] *= weights / peak if peak > 0 else 0
-    if return_signal:
-        signal_shape = (*shape, 2, nt) if method == "apertures" else (*shape, nt)
-        return pd[:, 0].reshape(shape), signal.reshape(signal_shape)
-    return np.ascontiguousarray(pd[:, 0]).reshape(shape), signal
+        power = power * (weights / peak if peak > 0 else 0)
+    power = np.ascontiguousarray(power).reshape(acq.grid_shape)
+    if not return_signal:
+        return power, signal
+    return power, signal.reshape((*acq.grid_shape, 2, nt) if planes == 2 else (*acq.grid_shape, nt))
 
 
 def ensemble_pd_from_channels(rc, cr, angles, t_start, grid, geom: RCAGeometry, *, method: Method = "opw", k: int = 2,

@@ -2,7 +2,7 @@
 
 Run in a container where the reference checkout is available:
 
-    python tests/golden/make_golden.py /path/to/rcabeam
+    python tests/golden/make_golden.py /path/to/rcabeam    (or RCABEAM_REFERENCE=/path/to/rcabeam)
 
 It imports ``rcabeam`` from ``<reference>/src`` (NumPy modules only: sim,
 clutter, power, opw, ensemble.opw_voxel_order, dmas, fmas, stsw) and writes
@@ -184,10 +184,29 @@ def stsw_cases(sim, stsw):
     return cases
 
 
+def scene_cases(sim):
+    """Channel IQ of single static point scatterers from the reference ``simulate_point``
+    (sim.py:131-189, Gaussian envelope, sigma_t = 0.15 us): the pulse model that the
+    scene forward model sums over scatterers."""
+    # Inputs are float32-exact: the forward-model kernel reads float32 fields.
+    f32 = lambda v: np.asarray(v, dtype=np.float32).astype(np.float64)  # noqa: E731
+    el_x, el_y = f32((np.arange(16) - 7.5) * 0.2e-3), f32((np.arange(16) - 7.5) * 0.18e-3)
+    geom = sim.RCAGeometry(el_x, el_y, c=1540.0, fs=20e6, f_demod=15e6, fnumber=None)
+    angles = f32(np.deg2rad(np.array([-8.0, 0.0, 5.0])))
+    points = f32([[0.3e-3, 4.0e-3, -0.2e-3], [-1.1e-3, 4.6e-3, 0.9e-3]])
+    cases = dict(el_x=el_x, el_y=el_y, angles=angles, points=points, nsamp=160, t_start=f32(4.4e-6))
+    for i, point in enumerate(points):
+        for config in ("RC", "CR"):
+            cases[f"point{i}_{config}"] = sim.simulate_point(geom, angles, tuple(point), 160, float(cases["t_start"]),
+                                                             config)
+    return cases
+
+
 def main(root: str) -> None:
     sim, clutter, ensemble, dmas = _import_reference(root)
     import rcabeam.stsw as stsw
 
+    np.savez_compressed(HERE / "scene.npz", **scene_cases(sim))
     np.savez_compressed(HERE / "stsw.npz", **stsw_cases(sim, stsw))
     np.savez_compressed(HERE / "das.npz", **das_cases(sim))
     np.savez_compressed(HERE / "clutter.npz", **clutter_cases(clutter))
@@ -198,4 +217,9 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import os
+
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RCABEAM_REFERENCE")
+    if not root:
+        sys.exit("usage: make_golden.py <reference checkout> (or set RCABEAM_REFERENCE)")
+    main(root)

@@ -250,3 +250,35 @@ def test_scale_max_abs_matches_torch(n, offset):
     _lib.call("rcabeam_clutter_scale_device", x.data_ptr(), n, 0, scale.data_ptr())
     want = torch.view_as_real(x).abs().max().double()
     assert float(scale.item()) == float(want.item()) == 7.5
+
+
+@pytest.mark.parametrize("rows,nt", [(1, 2), (31, 8), (33, 64), (1000, 128), (70001, 200), (257, 256), (65, 258),
+                                     (4097, 400), (40, 512), (5, 199)])
+@pytest.mark.parametrize("k,mode", [(3, 1), (3, 3), (1, 0), (4, 2), (2, 1)])
+@pytest.mark.parametrize("offset", [0, 1])
+def test_projection_rows_match_float64(rows, nt, k, mode, offset):
+    """rcabeam_project_device on complex64 rows (the streamed kernel for even frame counts and
+    16-byte aligned rows; the warp-per-row kernel for odd counts or an 8-byte offset) against
+    float64 NumPy: power to 1e-12 relative, written rows to float32 rounding."""
+    rng = np.random.default_rng(rows + nt + k)
+    host = (rng.normal(size=(rows, nt)) + 1j * rng.normal(size=(rows, nt))).astype(np.complex64)
+    host[:, :] += 50 * np.exp(2j * np.pi * 0.01 * np.arange(nt))  # a strong common component
+    q, _ = np.linalg.qr(rng.normal(size=(nt, k)) + 1j * rng.normal(size=(nt, k)))
+    flat = torch.zeros(rows * nt + 1, dtype=torch.complex64, device="cuda")
+    iq = flat[offset:offset + rows * nt]
+    iq.copy_(torch.from_numpy(host.ravel()))
+    vec = _dev(np.asfortranarray(q).ravel(order="F"))
+    out = torch.zeros(rows * nt, dtype=torch.complex64, device="cuda") if mode & 2 else None
+    power = torch.zeros(rows, dtype=torch.float64, device="cuda")
+    _lib.call("rcabeam_project_device", iq.data_ptr(), None if out is None else out.data_ptr(), power.data_ptr(),
+              rows, nt, 0, vec.data_ptr(), k, mode)
+    x = host.astype(np.complex128)
+    y = x @ q
+    part = y @ q.conj().T
+    resid = x - part if mode & 1 else part
+    want = (np.sum(np.abs(resid) ** 2, axis=1) if mode & 1 else np.sum(np.abs(y) ** 2, axis=1)) / nt
+    got = power.cpu().numpy()
+    np.testing.assert_allclose(got, want, rtol=1e-11, atol=1e-12 * want.max())
+    if out is not None:
+        np.testing.assert_allclose(out.cpu().numpy().reshape(rows, nt), resid, rtol=0,
+                                   atol=2e-6 * np.abs(resid).max() + 1e-6)

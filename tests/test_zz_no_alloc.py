@@ -1,9 +1,9 @@
 """The no-allocation ensemble entry point against the workspace entry point.
 
 ``rcabeam_ensemble_static_device`` serves callers that cannot allocate device
-memory (graph-recording code, fixed-budget acquisition loops, hosts whose
-allocator belongs to another runtime): its scratch lives in a fixed array inside
-the library.  This file runs last (collection order) so that, if it fails, a
+memory (acquisition loops whose device memory budget is fixed when the scanner
+starts, plugins whose host application owns the device allocator): its scratch
+lives in a fixed array inside the library.  This file runs last (collection order) so that, if it fails, a
 ``-x`` run has already run every other test.
 """
 
@@ -49,45 +49,69 @@ def _device_inputs(rc, cr, angles, grid, geom):
     f32 = lambda v: torch.from_numpy(np.ascontiguousarray(v, dtype=np.float32)).cuda()  # noqa: E731
     packed = []
     for raw in (rc, cr):
-        src = torch.from_numpy(raw).cuda()
+        src = torch.from_numpy(np.ascontiguousarray(raw)).cuda()
         dst = torch.empty(ns * nc * na * nt * 8, dtype=torch.uint8, device="cuda")
         _lib.call("rcabeam_pack_ensemble_device", src.data_ptr(), dst.data_ptr(), ns, nc, na, nt)
         packed.append(dst)
     return packed, f32(scan_coords(grid)), f32(geom.x_el), f32(geom.y_el), f32(angles), f32([4e-6] * na)
 
 
-@pytest.mark.parametrize("method", [0, 1, 5])
-def test_static_entry_matches_workspace_entry_twice(method):
-    rc, cr, angles, grid, geom = _case()
+def _compare(method, rc, cr, angles, grid, geom):
+    """Static entry point vs rcabeam_ensemble_device on the same inputs, two calls in a row."""
     ns, nc, na, nt = rc.shape
     (prc, pcr), scan, xe, ye, an, st = _device_inputs(rc, cr, angles, grid, geom)
     nv = scan.shape[0]
     planes = 2 if method == 5 else 1
+    with_signal = method in (0, 1, 5)
     consts = (float(geom.c), float(geom.fs), float(geom.f_demod), float(geom.fnumber))
     ref_pd = torch.empty((nv, 2), device="cuda")
-    ref_sig = torch.empty((nv * planes, nt), dtype=torch.complex64, device="cuda")
+    ref_sig = torch.empty((nv * planes, nt), dtype=torch.complex64, device="cuda") if with_signal else None
     ws = torch.empty(_cuda_impl.workspace_bytes(nv, nc, na), dtype=torch.uint8, device="cuda")
     _lib.call("rcabeam_ensemble_device", prc.data_ptr(), pcr.data_ptr(), scan.data_ptr(), xe.data_ptr(), ye.data_ptr(),
-              an.data_ptr(), st.data_ptr(), ref_pd.data_ptr(), ref_sig.data_ptr(), None, None, ws.data_ptr(), ns, nc,
-              na, nt, nv, *consts, method, 2)
+              an.data_ptr(), st.data_ptr(), ref_pd.data_ptr(), ref_sig.data_ptr() if with_signal else None, None, None,
+              ws.data_ptr(), ns, nc, na, nt, nv, *consts, method, 2)
     torch.cuda.synchronize()
-    expected_pd, expected_sig = ref_pd[:, 0].cpu().numpy(), ref_sig.cpu().numpy()
+    expected_pd = ref_pd[:, 0].cpu().numpy()
+    expected_sig = ref_sig.cpu().numpy() if with_signal else None
     pd = torch.empty((nv, 2), device="cuda")
-    sig = torch.empty((nv * planes, nt), dtype=torch.complex64, device="cuda")
+    sig = torch.empty((nv * planes, nt), dtype=torch.complex64, device="cuda") if with_signal else None
     for _ in range(2):  # two calls in a row share the library's scratch
         pd.fill_(float("nan"))
-        sig.fill_(float("nan"))
+        if with_signal:
+            sig.fill_(float("nan"))
         torch.cuda.synchronize()
         before = torch.cuda.memory_stats().get("allocation.all.allocated", 0)
+        free_before = torch.cuda.mem_get_info()[0]
         _lib.call("rcabeam_ensemble_static_device", prc.data_ptr(), pcr.data_ptr(), scan.data_ptr(), xe.data_ptr(),
-                  ye.data_ptr(), an.data_ptr(), st.data_ptr(), pd.data_ptr(), sig.data_ptr(), ns, nc, na, nt, nv,
-                  *consts, method)
+                  ye.data_ptr(), an.data_ptr(), st.data_ptr(), pd.data_ptr(), sig.data_ptr() if with_signal else None,
+                  ns, nc, na, nt, nv, *consts, method)
         torch.cuda.synchronize()
+        # Neither torch's allocator nor the driver gave out memory during the call (the driver
+        # figure catches a cudaMalloc inside the library; 2 MiB of slack for driver bookkeeping).
         assert torch.cuda.memory_stats().get("allocation.all.allocated", 0) == before
-        assert rel_l2(sig.cpu().numpy(), expected_sig) <= 1e-5
-        np.testing.assert_allclose(sig.cpu().numpy(), expected_sig, rtol=0, atol=2e-5 * np.abs(expected_sig).max())
+        assert torch.cuda.mem_get_info()[0] >= free_before - (2 << 20)
+        if with_signal:
+            assert rel_l2(sig.cpu().numpy(), expected_sig) <= 1e-5
+            np.testing.assert_allclose(sig.cpu().numpy(), expected_sig, rtol=0,
+                                       atol=2e-5 * np.abs(expected_sig).max())
         if method != 5:
             assert rel_l2(pd[:, 0].cpu().numpy(), expected_pd) <= 1e-5
+
+
+@pytest.mark.parametrize("method", [0, 1, 2, 3, 5])
+def test_static_entry_matches_workspace_entry_twice(method):
+    _compare(method, *_case())
+
+
+@pytest.mark.parametrize("method", [0, 3])
+def test_static_entry_at_its_voxel_limit(method):
+    """262144 voxels (the documented limit): the traversal-order sort fits the fixed scratch."""
+    size = ctypes.c_size_t(0)
+    assert _lib.lib().rcabeam_voxel_order_workspace_bytes(MAX_VOXELS, ctypes.byref(size)) == 0
+    assert 0 < size.value <= 8 << 20
+    rc, cr, angles, grid, geom = _case(frames=8, nx=64, nz=64, ny=64)
+    _compare(method, rc[:, :8], cr[:, :8], angles, grid,
+             RCAGeometry(geom.x_el[:8], geom.y_el[:8], c=geom.c, fs=geom.fs, f_demod=geom.f_demod, fnumber=1.0))
 
 
 def test_static_entry_rejects_too_many_voxels():
