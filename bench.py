@@ -438,6 +438,7 @@ def run_batching(args) -> dict:
                                             "p99": round(float(np.percentile(seq_done, 99)), 1)}},
         "power_rel_l2_batch_vs_sequential_max": worst,
         "autotune": {**choice, "seconds": round(tune_s, 2)},
+        "launches": "one persistent kernel per method (own register budget), forked streams, one CUDA graph",
         "latency_definition": "completion time since the queue started (device global timer for the persistent "
                               "kernel, CUDA events for sequential launches)",
         "dtype": "f32 math on c64 packed IQ (float64 geometry)", "data": "synthetic seeded complex Gaussian channels",
@@ -445,7 +446,7 @@ def run_batching(args) -> dict:
                                "(central block of the 128-wide grid), frames {50,100,200,400}, 128 ch, "
                                "angles {5,7,11}, ns 512, 50% OPW / 25% XDoppler / 25% DMAS-CCF-ACF",
                    "seed": args.seed, "ensembles": shapes},
-        "clocks": clocks, "gpu_launches": steps,
+        "clocks": clocks, "gpu_launches": steps * len(queue.parts),
     }
 
 

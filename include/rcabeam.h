@@ -159,10 +159,14 @@ rcabeam_status rcabeam_pack_ensemble_split_device(const void* source, void* hi, 
                                                   size_t nc, size_t na, size_t nt);
 
 /* OPW IQ and power on tcgen05 tensor cores (interpolation as a banded GEMM
- * over 64-voxel tiles).  precision 0: rc_hi / cr_hi are FP16-packed channels
- * (rcabeam_pack_ensemble_fp16_device), rc_lo / cr_lo unused; precision 1:
- * BF16 hi / lo planes from rcabeam_pack_ensemble_split_device.  Coefficients
- * are split into hi + lo halves; accumulation is float32.  pd, signal and
+ * over 64-voxel tiles).  precision bit 0 clear: rc_hi / cr_hi are FP16-packed
+ * channels (rcabeam_pack_ensemble_fp16_device), rc_lo / cr_lo unused; bit 0
+ * set: BF16 hi / lo planes from rcabeam_pack_ensemble_split_device.  Bit 1 set:
+ * every tile walks its channels in one fixed order, so repeated calls give
+ * bit-identical results (clear: each tile starts where the other SMs are,
+ * which keeps their sample windows in L2 together but makes the order of the
+ * float32 sums, and their last bits, depend on timing).  Coefficients are
+ * split into hi + lo halves; accumulation is float32.  pd, signal and
  * geometry_workspace are as for rcabeam_ensemble_device (method 0).  Requires
  * nt % 4 == 0 and 16-byte aligned planes (RCABEAM_ERROR_ARGUMENT otherwise).
  * rcabeam_opw_fp16_device uses this kernel whenever its inputs qualify. */
@@ -209,6 +213,14 @@ rcabeam_status rcabeam_heevd_device(double* gram, double* eigenvalues, size_t nt
  * nt <= 512. */
 rcabeam_status rcabeam_project_device(const void* iq, void* out, double* power, size_t rows, size_t nt,
                                       int complex128, const double* vectors, size_t k, int mode);
+
+/* One float64 subspace-iteration step (complex64 rows): z (device, column-major
+ * nt x k complex128, zeroed by the caller) += X^H (X V) for the k <= 4
+ * column-major (nt x k) complex128 vectors V, nt <= 512.  Orthonormalizing z
+ * refines dominant Gram eigenvectors from a reduced-precision Gram against the
+ * exact float64 Gram, without forming it. */
+rcabeam_status rcabeam_refine_vectors_device(const void* iq, size_t rows, size_t nt, const double* vectors,
+                                             size_t k, double* z);
 
 /* Bytes of geometry_workspace that rcabeam_ensemble_device / rcabeam_opw_fp16_device
  * actually use for nv voxels (at most the documented 2*nv*(nc+na) float4).  A
@@ -330,6 +342,14 @@ rcabeam_status rcabeam_voxel_order_workspace_bytes(size_t nv, size_t* bytes);
  * radix-sorted) of nv voxels into order (nv unsigned), on the default stream. */
 rcabeam_status rcabeam_voxel_order_device(const float* scan, size_t nv, unsigned* order, void* workspace,
                                           size_t workspace_bytes);
+
+/* Failure-path self-test of the bounded waits (extension; no counterpart in the
+ * reference): one CTA of four warps waits, limit_ns at most (<= 2 s), on an
+ * mbarrier that nothing arrives on, with the same wait routine as the
+ * staging pipelines.  Each wait gives up, sets the device error word to `code`
+ * (> 0; read it with rcabeam_device_error) and returns; *gave_up (device int,
+ * zeroed by the caller) counts the waits that gave up.  The context stays usable. */
+rcabeam_status rcabeam_wait_selftest_device(unsigned long long limit_ns, int code, int* gave_up);
 
 /* Reads and clears the device error word set by a kernel whose bounded wait
  * gave up (0 = no error).  Synchronizes the device. */

@@ -42,6 +42,7 @@ SIGNATURES: dict[str, list] = {
     "rcabeam_heevd_workspace_bytes": [Z, ctypes.POINTER(c_size_t)],
     "rcabeam_heevd_device": [P, P, Z, P, Z, P],
     "rcabeam_project_device": [P, P, P, Z, Z, I, P, Z, I],
+    "rcabeam_refine_vectors_device": [P, Z, Z, P, Z, P],
     "rcabeam_ensemble_static_device": [P, P, P, P, P, P, P, P, P, Z, Z, Z, Z, Z, F, F, F, F, I],
     "rcabeam_ensemble_workspace_bytes": [Z, Z, Z, ctypes.POINTER(c_size_t)],
     "rcabeam_opw_offsets_forward_device": [P, P, P, P, Z, P, P, P, P, P, D, F, F, F, Z, Z, Z, Z, Z, Z, P, P, I],
@@ -54,6 +55,7 @@ SIGNATURES: dict[str, list] = {
     "rcabeam_simulate_scene_device": [P, Z, P, P, P, P, Z, Z, Z, Z, I, D, D, D, D, D, D],
     "rcabeam_voxel_order_workspace_bytes": [Z, ctypes.POINTER(c_size_t)],
     "rcabeam_voxel_order_device": [P, Z, P, P, Z],
+    "rcabeam_wait_selftest_device": [ctypes.c_ulonglong, I, P],
     "rcabeam_device_error": [ctypes.POINTER(c_int)],
 }
 

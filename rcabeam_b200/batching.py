@@ -1,16 +1,21 @@
-"""Batching form: a queue of uneven ensembles through one persistent kernel.
+"""Batching form: a queue of uneven ensembles through persistent kernels under one CUDA graph.
 
 ``BatchQueue`` holds device-resident ensembles (packed RC/CR channels, grid,
-geometry, method) and reconstructs all of them with one launch of the
-persistent batch kernel (``rcabeam_batch_run_device``): OPW and XDoppler
-tiles run the TMA-staged pipeline, DMAS-CCF-ACF voxel blocks the nonlinear
-beamformer, items are taken from a global counter in queue order.  The launch
-(counter and power clears + the kernel) is captured once into a CUDA graph and
-replayed.  ``autotune`` picks, per ensemble shape class, the frame chunk of
-the staged pipeline and, for the queue, the resident CTAs per SM, by timing
-candidates on bounded samples of the ensembles.  Per-ensemble completion
-times come from the kernel (global timer), so latencies are measured on the
-device.
+geometry, method).  The queue is split by method into sub-queues, and each
+sub-queue is reconstructed by one launch of the persistent batch kernel
+(``rcabeam_batch_run_device``) with its own register budget (resident CTAs
+per SM): OPW and XDoppler tiles run the TMA-staged pipeline at one budget,
+DMAS-CCF-ACF's two-pass pipeline at another.  One register budget for all three
+methods made the single persistent launch slower than sequential launches
+(the OPW / XDoppler consumers spill at DMAS's budget, DMAS loses latency
+hiding at theirs).  The sub-queue launches run on forked streams and are
+captured together into one CUDA graph; within a launch, persistent CTAs take
+items from a global counter in queue order, so small and large ensembles
+share the GPU without launch gaps or per-ensemble tails.  ``autotune`` picks,
+per ensemble shape class, the frame chunk of the staged pipeline and, per
+method, the resident CTAs per SM, by timing candidates on bounded samples of
+the ensembles.  Per-ensemble completion times come from the kernels (global
+timer), so latencies are measured on the device.
 
 Methods: "opw" (power of the coherent sum), "xdoppler" (|mean r conj(q)|) and
 "dmas" (DMAS-CCF-ACF), as in ``ensemble_pd_from_channels`` (reference
@@ -116,35 +121,62 @@ class Ensemble:
         return self.tensors["pd"][:, 0]
 
 
-class BatchQueue:
-    """A prepared queue: device table, completion-time buffer, optional CUDA graph."""
+class _SubQueue:
+    """The ensembles of one method: device table, completion times, register budget."""
 
-    def __init__(self, ensembles, *, ctas_per_sm: int = 1, voxel_limit: int | None = None):
-        self.lib = _declare()
-        self.ensembles = list(ensembles)
-        self.ctas_per_sm = ctas_per_sm
-        device = self.ensembles[0].rc.device
-        n = len(self.ensembles)
+    def __init__(self, lib, indices, ensembles, ctas_per_sm: int, voxel_limit: int | None, device):
+        self.lib = lib
+        self.indices = indices
+        n = len(ensembles)
         self.list = (BatchEnsembleC * n)(*[e.descriptor(voxels=None if voxel_limit is None else
-                                                       min(voxel_limit, e.voxels)) for e in self.ensembles])
+                                                       min(voxel_limit, e.voxels)) for e in ensembles])
         size = ctypes.c_size_t(0)
-        _lib.check(self.lib.rcabeam_batch_table_bytes(n, self.list, ctypes.byref(size)), "batch_table_bytes")
+        _lib.check(lib.rcabeam_batch_table_bytes(n, self.list, ctypes.byref(size)), "batch_table_bytes")
         self.table = torch.empty(int(size.value) + 256, dtype=torch.uint8, device=device)
         self.base = (256 - self.table.data_ptr() % 256) % 256
         self.table_bytes = int(size.value)
-        _lib.check(self.lib.rcabeam_batch_prepare(n, self.list, self.table.data_ptr() + self.base, self.table_bytes),
+        _lib.check(lib.rcabeam_batch_prepare(n, self.list, self.table.data_ptr() + self.base, self.table_bytes),
                    "batch_prepare")
         self.times = torch.zeros(n + 1, dtype=torch.int64, device=device)
+        self.ctas_per_sm = ctas_per_sm
+
+    def launch(self, stream) -> None:
+        _lib.check(self.lib.rcabeam_batch_run_device(len(self.indices), self.list, self.table.data_ptr() + self.base,
+                                                     self.table_bytes, self.times.data_ptr(), self.ctas_per_sm,
+                                                     ctypes.c_void_p(stream.cuda_stream)), "batch_run")
+
+
+class BatchQueue:
+    """A prepared queue: one sub-queue per method, completion-time buffers, optional CUDA graph.
+
+    ``ctas_per_sm`` is an int (every method) or a {method: int} map (the autotuner's choice)."""
+
+    def __init__(self, ensembles, *, ctas_per_sm=1, voxel_limit: int | None = None):
+        self.lib = _declare()
+        self.ensembles = list(ensembles)
+        device = self.ensembles[0].rc.device
+        budget = ctas_per_sm if isinstance(ctas_per_sm, dict) else {m: int(ctas_per_sm) for m in METHODS}
+        # Longest-running methods first: later launches fill the SMs that earlier ones leave idle.
+        self.parts = []
+        for method in ("dmas", "opw", "xdoppler"):
+            idx = [i for i, e in enumerate(self.ensembles) if e.method == method]
+            if idx:
+                self.parts.append(_SubQueue(self.lib, idx, [self.ensembles[i] for i in idx], int(budget[method]),
+                                            voxel_limit, device))
+        self.streams = [torch.cuda.Stream(device) for _ in self.parts]
         self.graph = None
 
     def launch(self, stream: torch.cuda.Stream | None = None) -> None:
-        s = torch.cuda.current_stream() if stream is None else stream
-        _lib.check(self.lib.rcabeam_batch_run_device(len(self.ensembles), self.list, self.table.data_ptr() + self.base,
-                                                     self.table_bytes, self.times.data_ptr(), self.ctas_per_sm,
-                                                     ctypes.c_void_p(s.cuda_stream)), "batch_run")
+        """Fork the sub-queue launches onto their streams from ``stream`` and join them back."""
+        main = torch.cuda.current_stream() if stream is None else stream
+        for part, side in zip(self.parts, self.streams):
+            side.wait_stream(main)
+            part.launch(side)
+        for side in self.streams:
+            main.wait_stream(side)
 
     def capture(self) -> None:
-        """Record the launch into a CUDA graph (first run warms up outside the capture)."""
+        """Record the launches into one CUDA graph (the first run warms up outside the capture)."""
         side = torch.cuda.Stream()
         side.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(side):
@@ -162,9 +194,13 @@ class BatchQueue:
             self.launch()
 
     def completion_ms(self) -> np.ndarray:
-        """Per-ensemble completion time since the kernel started (device clock), ms."""
-        t = self.times.cpu().numpy().astype(np.int64)
-        return (t[1:] - t[0]) / 1e6
+        """Per-ensemble completion time since the first sub-queue kernel started (device clock), ms."""
+        times = [part.times.cpu().numpy().astype(np.int64) for part in self.parts]
+        start = min(t[0] for t in times)
+        out = np.empty(len(self.ensembles))
+        for part, t in zip(self.parts, times):
+            out[part.indices] = (t[1:] - start) / 1e6
+        return out
 
 
 def _sample(e: Ensemble, tiles: int) -> int:
@@ -172,12 +208,12 @@ def _sample(e: Ensemble, tiles: int) -> int:
 
 
 def autotune(ensembles, *, sample_tiles: int = 148 * 2, repeats: int = 2, cache: dict | None = None) -> dict:
-    """Frame chunk per shape class (staged methods) and CTAs per SM for the queue.
+    """Frame chunk per shape class (staged methods) and CTAs per SM per method.
 
     Each candidate runs the persistent kernel on a bounded sample (the first
     ``sample_tiles`` tiles of one ensemble of the class in traversal order) and
     is timed with CUDA events; the fastest per class is written back into the
-    ensembles.  Returns {class: frames_per_chunk, "ctas_per_sm": k}.
+    ensembles.  Returns {class: frames_per_chunk, "ctas_per_sm": {method: k}}.
     """
     cache = {} if cache is None else cache
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -212,11 +248,16 @@ def autotune(ensembles, *, sample_tiles: int = 148 * 2, repeats: int = 2, cache:
     for e in ensembles:
         e.frames_per_chunk = cache[(e.method, e.shape[2], e.shape[3])]
     if "ctas_per_sm" not in cache:
-        reps = list(classes.values())
-        results = {}
-        for k in (1, 2, 3):
-            results[k] = timed(BatchQueue(reps, ctas_per_sm=k, voxel_limit=64 * sample_tiles))
-        cache["ctas_per_sm"] = min(results, key=results.get)
+        # Register budget per method, on that method's shape classes.
+        budgets = {}
+        for method in METHODS:
+            reps = [e for key, e in classes.items() if key[0] == method]
+            if not reps:
+                budgets[method] = 1
+                continue
+            results = {k: timed(BatchQueue(reps, ctas_per_sm=k, voxel_limit=64 * sample_tiles)) for k in (1, 2, 3)}
+            budgets[method] = min(results, key=results.get)
+        cache["ctas_per_sm"] = budgets
     return {**{str(k): v for k, v in cache.items() if k != "ctas_per_sm"}, "ctas_per_sm": cache["ctas_per_sm"]}
 
 

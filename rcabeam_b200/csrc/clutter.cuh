@@ -504,5 +504,96 @@ __global__ void __launch_bounds__(PipeShape<G>::kThreads, 1)
   }
 }
 
+// One float64 subspace-iteration step for the dominant temporal vectors:
+// z += X^H (X V) over rows [r0, r1) of the Casorati matrix, V = nt x k
+// (column-major complex128, k <= kRefineMax), z = nt x k (column-major
+// complex128, accumulated with atomics).  The Gram of the tensor-core
+// precisions is rounded to 16-bit / TF32 operands; multiplying the current
+// vectors by the exact float64 Gram (without forming it) and re-orthonormalizing
+// shrinks their error by the gap ratio lambda_{k+1} / lambda_k.
+// Per CTA: blocks of kRefineRows rows are staged in shared memory (complex64);
+// each warp forms y = x V for two rows (float64 dot products, warp
+// reductions), then every thread accumulates conj(x_t) y_c for its frames t.
+constexpr int kRefineMax = 4;
+constexpr int kRefineRows = 16;
+constexpr int kRefineThreads = 256;
+
+__global__ void __launch_bounds__(kRefineThreads)
+    refine_vectors(const float2* __restrict__ x, size_t rows, int nt, const double2* __restrict__ vec, int k,
+                   double* __restrict__ z) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double2* vs = reinterpret_cast<double2*>(smem);                 // [k][nt]
+  double2* ys = vs + size_t(kRefineMax) * nt;                     // [rows][k]
+  float2* xs = reinterpret_cast<float2*>(ys + kRefineRows * kRefineMax);  // [rows][nt]
+  for (int i = threadIdx.x; i < k * nt; i += blockDim.x) vs[i] = vec[i];
+  const size_t per = (rows + gridDim.x - 1) / gridDim.x;
+  const size_t r0 = size_t(blockIdx.x) * per, r1 = min(rows, r0 + per);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int kFramesPerThread = 2;  // nt <= 512 = 2 x 256
+  double zr[kFramesPerThread][kRefineMax], zi[kFramesPerThread][kRefineMax];
+#pragma unroll
+  for (int f = 0; f < kFramesPerThread; ++f)
+#pragma unroll
+    for (int c = 0; c < kRefineMax; ++c) zr[f][c] = zi[f][c] = 0.0;
+  for (size_t b = r0; b < r1; b += kRefineRows) {
+    const int nr = int(min(size_t(kRefineRows), r1 - b));
+    __syncthreads();  // the previous block's rows and coordinates are no longer read
+    for (int i = threadIdx.x; i < nr * nt; i += blockDim.x) xs[i] = x[b * size_t(nt) + i];
+    __syncthreads();
+    // Coordinates y[r][c] = sum_t x[r][t] v_c[t] (two rows per warp).
+    for (int rr = 2 * warp; rr < 2 * warp + 2; ++rr) {
+      for (int c = 0; c < k; ++c) {
+        double yr = 0.0, yi = 0.0;
+        if (rr < nr) {
+          for (int t = lane; t < nt; t += 32) {
+            const float2 a = xs[rr * nt + t];
+            const double2 v = vs[c * nt + t];
+            yr = fma(double(a.x), v.x, fma(-double(a.y), v.y, yr));
+            yi = fma(double(a.x), v.y, fma(double(a.y), v.x, yi));
+          }
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+          yr += __shfl_xor_sync(0xffffffffu, yr, off);
+          yi += __shfl_xor_sync(0xffffffffu, yi, off);
+        }
+        if (lane == 0) ys[rr * kRefineMax + c] = make_double2(rr < nr ? yr : 0.0, rr < nr ? yi : 0.0);
+      }
+    }
+    __syncthreads();
+    // z[t][c] += conj(x[r][t]) y[r][c].
+#pragma unroll
+    for (int f = 0; f < kFramesPerThread; ++f) {
+      const int t = threadIdx.x + f * kRefineThreads;
+      if (t < nt) {
+        for (int r = 0; r < nr; ++r) {
+          const float2 a = xs[r * nt + t];
+          const double ar = double(a.x), ai = double(a.y);
+#pragma unroll
+          for (int c = 0; c < kRefineMax; ++c) {
+            if (c < k) {
+              const double2 y = ys[r * kRefineMax + c];
+              zr[f][c] = fma(ar, y.x, fma(ai, y.y, zr[f][c]));
+              zi[f][c] = fma(ar, y.y, fma(-ai, y.x, zi[f][c]));
+            }
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < kFramesPerThread; ++f) {
+    const int t = threadIdx.x + f * kRefineThreads;
+    if (t < nt) {
+#pragma unroll
+      for (int c = 0; c < kRefineMax; ++c) {
+        if (c < k) {
+          atomicAdd(z + 2 * (size_t(c) * nt + t), zr[f][c]);
+          atomicAdd(z + 2 * (size_t(c) * nt + t) + 1, zi[f][c]);
+        }
+      }
+    }
+  }
+}
+
 }  // namespace clutter
 }  // namespace rcb

@@ -124,17 +124,33 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Waits for the phase with the given parity; false (and *err set) after the limit.
-__device__ __noinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
+// Waits for the phase with the given parity; false (and *err set) after `limit_ns`.
+__device__ __noinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code,
+                                       unsigned long long limit_ns = kWaitLimitNs) {
   if (mbar_test(bar, parity)) return true;
   unsigned long long start = global_ns();
   for (uint32_t i = 0;; ++i) {
     if (mbar_test(bar, parity)) return true;
-    if ((i & 255u) == 255u && global_ns() - start > kWaitLimitNs) {
+    if ((i & 255u) == 255u && global_ns() - start > limit_ns) {
       if (err) atomicCAS(err, 0, code);
       return false;
     }
   }
+}
+
+// Failure-path check of the bounded waits: every warp of one CTA waits, with
+// `limit_ns`, on an mbarrier that nothing arrives on, exactly as a pipeline
+// stage whose producer never delivers.  Each wait gives up, records `code` in
+// the device error word and the kernel returns; *gave_up counts the waits that
+// returned false.
+__global__ void wait_selftest(int* err, int code, unsigned long long limit_ns, int* gave_up) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0 && !mbar_wait(&bar, 0, err, code, limit_ns)) atomicAdd(gave_up, 1);
 }
 
 // mbar_wait with the already-complete case inline (no call on the fast path).

@@ -379,14 +379,8 @@ static bool use_tm_kernel() {
   return !(v && std::string(v) == "smem");
 }
 
-static bool deterministic_walk() {
-  const char* v = std::getenv("RCABEAM_DETERMINISTIC");
-  return v && v[0] == '1';
-}
-
 template <bool BF16X3>
 static rcabeam_status run_tc(tc::Args a) {
-  a.walk_fixed = deterministic_walk() ? 1 : 0;
   if (use_tm_kernel()) return run_tm<BF16X3>(a);
   const size_t nt = size_t(a.nt);
   // The deepest ring (one builder warp per stage) that fits shared memory.
@@ -774,6 +768,12 @@ rcabeam_status rcabeam_clutter_scale_device(const void* iq, size_t n, int comple
 // Tensor-core Gram (precision 2 = TF32, 3 = 3xBF16) of a complex64 Casorati
 // matrix: the rows x 2T float32 view as a 2-D tensor with 32 x 16 SWIZZLE_128B
 // boxes, one CTA per (unit, row slice).
+// RCABEAM_GRAM_KERNEL=staged selects the TMA-staged 3xBF16 Gram (a/b timing).
+static bool gram_staged_bf16() {
+  const char* v = std::getenv("RCABEAM_GRAM_KERNEL");
+  return v && std::string(v) == "staged";
+}
+
 static rcabeam_status gram_tc_launch(const void* iq, size_t rows, size_t nt, const double* scale, bool tf32,
                                      double* upper) {
   auto fn = encode_fn();
@@ -803,6 +803,15 @@ static rcabeam_status gram_tc_launch(const void* iq, size_t rows, size_t nt, con
          CU_TENSOR_MAP_INTERLEAVE_NONE, tf32 ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B : CU_TENSOR_MAP_SWIZZLE_128B,
          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return RCABEAM_ERROR_ARGUMENT;
+  if (!tf32 && !gram_staged_bf16()) {
+    // 3xBF16: converters load the rows from global memory (no TMA staging).
+    const size_t smem = std::max(gramtc::direct_smem_bytes(prm.nload_max), size_t(120) << 10);
+    auto kern = gramtc::gram_bf16_direct;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+      return RCABEAM_ERROR_CUDA;
+    kern<<<unsigned(prm.nunits * prm.slices), gramtc::kThreads, smem>>>(static_cast<const float*>(iq), prm);
+    return launch_status();
+  }
   // At least 120 KB keeps one CTA (and one 512-column TMEM allocation) per SM.
   const size_t smem = std::max(gramtc::smem_bytes(prm.nload_max), size_t(120) << 10);
   auto kern = tf32 ? gramtc::gram_tc<true> : gramtc::gram_tc<false>;
@@ -893,6 +902,25 @@ rcabeam_status rcabeam_project_device(const void* iq, void* out, double* power, 
   return launch_status();
 }
 
+rcabeam_status rcabeam_refine_vectors_device(const void* iq, size_t rows, size_t nt, const double* vectors,
+                                             size_t k, double* z) {
+  if (!iq || !vectors || !z || !rows || !nt || nt > 512 || !k || k > size_t(clutter::kRefineMax) ||
+      reinterpret_cast<uintptr_t>(iq) % 8 != 0)
+    return RCABEAM_ERROR_ARGUMENT;
+  const size_t smem = size_t(clutter::kRefineMax) * nt * 16 + size_t(clutter::kRefineRows) * clutter::kRefineMax * 16 +
+                      size_t(clutter::kRefineRows) * nt * 8;
+  if (cudaFuncSetAttribute(clutter::refine_vectors, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) !=
+      cudaSuccess)
+    return RCABEAM_ERROR_CUDA;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t blocks = std::min<size_t>(size_t(sms) * 4, (rows + clutter::kRefineRows - 1) / clutter::kRefineRows);
+  clutter::refine_vectors<<<unsigned(blocks), clutter::kRefineThreads, smem>>>(
+      static_cast<const float2*>(iq), rows, int(nt), reinterpret_cast<const double2*>(vectors), int(k), z);
+  return launch_status();
+}
+
 rcabeam_status rcabeam_ensemble_workspace_bytes(size_t nv, size_t nc, size_t na, size_t* bytes) {
   if (!bytes || !nv || !nc || !na) return RCABEAM_ERROR_ARGUMENT;
   size_t need = order_bytes(nv, nullptr);
@@ -907,6 +935,14 @@ rcabeam_status rcabeam_ensemble_static_device(const void* rc, const void* cr, co
                                               float c, float fs, float fd, float fn, int method) {
   return ensemble_static(rc, cr, scan, xe, ye, angles, starts, pd, signal, ns, nc, na, nt, nv, c, fs, fd, fn,
                          method);
+}
+
+rcabeam_status rcabeam_wait_selftest_device(unsigned long long limit_ns, int code, int* gave_up) {
+  if (!gave_up || code <= 0 || limit_ns == 0 || limit_ns > kWaitLimitNs) return RCABEAM_ERROR_ARGUMENT;
+  int* err = device_error_ptr();
+  if (!err) return RCABEAM_ERROR_CUDA;
+  wait_selftest<<<1, 128>>>(err, code, limit_ns, gave_up);
+  return launch_status();
 }
 
 rcabeam_status rcabeam_device_error(int* code) {
@@ -965,12 +1001,13 @@ rcabeam_status rcabeam_opw_tc_device(const void* rc_hi, const void* rc_lo, const
                                      float fd, float fn, int precision) {
   if (!rc_hi || !cr_hi || !scan || !xe || !ye || !angles || !starts || !pd || !geometry_workspace || ns < 2 ||
       !nc || !na || !nt || !nv || c <= 0 || fs <= 0 || !std::isfinite(c) || !std::isfinite(fs) ||
-      !std::isfinite(fd) || !std::isfinite(fn) || (precision != 0 && precision != 1))
+      !std::isfinite(fd) || !std::isfinite(fn) || precision < 0 || precision > 3)
     return RCABEAM_ERROR_ARGUMENT;
   if (ns > INT32_MAX || nc * na > INT32_MAX || nt > INT32_MAX || nv > size_t(INT32_MAX) - tc::kVox || na > 4096)
     return RCABEAM_ERROR_ARGUMENT;
+  const bool bf16x3 = precision & 1;
   const void* planes[4] = {rc_hi, cr_hi, rc_lo, cr_lo};
-  if (!tc_eligible(planes, precision == 1 ? 4 : 2, nt)) return RCABEAM_ERROR_ARGUMENT;
+  if (!tc_eligible(planes, bf16x3 ? 4 : 2, nt)) return RCABEAM_ERROR_ARGUMENT;
   if (cudaMemsetAsync(pd, 0, 2 * nv * sizeof(float), 0) != cudaSuccess) return RCABEAM_ERROR_CUDA;
   tc::Args t{};
   t.x_hi[0] = rc_hi;
@@ -995,7 +1032,8 @@ rcabeam_status rcabeam_opw_tc_device(const void* rc_hi, const void* rc_lo, const
   t.fd = fd;
   t.fn = fn;
   t.err = device_error_ptr();
-  return precision == 1 ? run_tc<true>(t) : run_tc<false>(t);
+  t.walk_fixed = (precision & 2) ? 1 : 0;
+  return bf16x3 ? run_tc<true>(t) : run_tc<false>(t);
 }
 
 rcabeam_status rcabeam_opw_fp16_device(const void* rc, const void* cr, const float* scan, const float* xe,

@@ -35,11 +35,20 @@ _CHANNEL_STAGES = ("gram", "eig", "filter", "pack", "das")
 
 
 class FilteredOpw:
-    """Fixed-shape filtered-OPW pipeline: ``run(rc, cr) -> (nx, nz, ny)`` float64 filtered power."""
+    """Fixed-shape filtered-OPW pipeline: ``run(rc, cr) -> (nx, nz, ny)`` float64 filtered power.
+
+    At a tensor-core Gram precision (``"tf32"``, ``"bf16x3"``) the discarded leading
+    vectors get one float64 subspace-iteration step against the exact Gram
+    (``refine``, default on when the smaller projector is ranks [0, rank_start)).
+    ``iq_storage="bf16x2"`` runs the tensor-core DAS on split-BF16 planes; with
+    ``deterministic=True`` its channel walk is fixed, so reruns are bit-identical
+    (by default each tile starts where the other SMs are, which keeps their
+    windows in L2 together and makes the last bits of the float32 sums timing
+    dependent)."""
 
     def __init__(self, channel_shape, angles, t_start, grid, geom: RCAGeometry, *, rank_start: int = 3,
                  rank_stop: int | None = None, precision: str = "complex128", iq_storage: str = "float32",
-                 group=None, domain: str = "beamformed"):
+                 group=None, domain: str = "beamformed", deterministic: bool = False, refine: bool | None = None):
         ns, nc, na, nt = (int(n) for n in channel_shape)
         self.shape = (len(grid[0]), len(grid[1]), len(grid[2]))
         self.channel_shape = (ns, nc, na, nt)
@@ -60,6 +69,8 @@ class FilteredOpw:
             raise ValueError("bf16x2 storage requires a frame count divisible by 4")
         self.storage = iq_storage
         self.half = iq_storage == "float16"
+        # Tensor-core DAS: fixed channel walk (bit-identical reruns) instead of the L2-aligned one.
+        self.deterministic = bool(deterministic)
         dev = torch.device("cuda", torch.cuda.current_device())
         self.device = dev
         scan = scan_coords(grid)
@@ -89,6 +100,14 @@ class FilteredOpw:
         self.subtract = stop - start > nt - (stop - start)
         self.k = (start + nt - stop) if self.subtract else (stop - start)
         self.vectors = torch.empty((max(self.k, 1), nt), dtype=torch.complex128, device=dev)
+        # Float64 subspace refinement of the discarded leading vectors (one X^H (X V) pass)
+        # when the Gram runs at a tensor-core precision; only when the smaller projector is
+        # the leading ranks [0, rank_start) (subtract mode, rank_stop = nt).
+        leading = self.subtract and stop == nt and 0 < self.k <= 4
+        self.refine = (precision in ("tf32", "bf16x3") if refine is None else bool(refine)) and leading
+        if self.refine and (domain != "beamformed" or group is not None):
+            self.refine = False
+        self.refined = torch.empty((max(self.k, 1), nt), dtype=torch.complex128, device=dev)
         self.events = [torch.cuda.Event(enable_timing=True) for _ in range(len(_STAGES) + 1)]
         self.last_das_event_ms = None
 
@@ -101,6 +120,16 @@ class FilteredOpw:
         ranks = torch.cat((desc[:start], desc[stop:])) if self.subtract else desc[start:stop]
         if self.k:
             torch.index_select(vt, 0, ranks, out=self.vectors[: self.k])
+
+    def _refine(self) -> None:
+        """One float64 subspace-iteration step: vectors <- orthonormal basis of X^H (X V) (no host sync)."""
+        k, nt = self.k, self.channel_shape[3]
+        z = self.refined[:k]
+        z.zero_()
+        _lib.call("rcabeam_refine_vectors_device", self.iq.data_ptr(), self.nv, nt, self.vectors.data_ptr(), k,
+                  z.data_ptr())
+        q, _ = torch.linalg.qr(z.transpose(0, 1))  # (nt, k), orthonormal columns spanning X^H X V
+        self.vectors[:k].copy_(q.transpose(0, 1))
 
     def run(self, rc: torch.Tensor, cr: torch.Tensor, after_inputs=None) -> torch.Tensor:
         """Filtered power of resident complex64 RC/CR channels ``(ns, nc, na, nt)``.
@@ -127,6 +156,8 @@ class FilteredOpw:
             self.power.zero_()
         else:
             self._select_vectors()
+            if self.refine:
+                self._refine()
             _lib.call("rcabeam_project_device", self.iq.data_ptr(), None, self.power.data_ptr(), self.nv,
                       self.channel_shape[3], 0, self.vectors.data_ptr(), self.k, 1 if self.subtract else 0)
         ev[5].record()
@@ -189,7 +220,7 @@ class FilteredOpw:
                       self.packed[1].data_ptr(), self.packed_lo[1].data_ptr(), self.scan.data_ptr(),
                       self.xe.data_ptr(), self.ye.data_ptr(), self.angles.data_ptr(), self.starts.data_ptr(),
                       self.pd.data_ptr(), signal, self.geometry.data_ptr(), ns, nc, na, nt, self.nv,
-                      *self.consts, 1)
+                      *self.consts, 1 | (2 if self.deterministic else 0))
         else:
             _cuda_impl.opw_from_packed(self.packed[0], self.packed[1], self.scan, self.xe, self.ye, self.angles,
                                        self.starts, self.pd, iq, self.geometry, ns, nc, na, nt, *self.consts,
@@ -272,7 +303,7 @@ class FilteredOpw:
         das = 1 if self.storage != "float32" and self.channel_shape[3] % 4 == 0 else 2
         if self.domain == "channel":  # scale x2, Gram x2, finish, projection x2, pack x2, order, DAS
             return 5 + 2 + 2 + 6 + das
-        return 2 + 6 + das + 4
+        return 2 + 6 + das + 4 + (1 if self.refine else 0)
 
 
 def synthetic_channels(shape, *, generator: torch.Generator, device, scale: float = 1.0):

@@ -82,13 +82,15 @@ def test_queue_matches_single_ensemble_path(chunk, ctas):
         assert rel_l2(e.power().cpu().numpy(), w.cpu().numpy()) <= 1e-5, e.method
     done = q.completion_ms()
     assert np.all(done > 0) and np.all(np.isfinite(done))
+    assert len(q.parts) == len({e.method for e in ens})  # one persistent launch per method
 
 
 def test_graph_replay_and_autotune():
     ens = _queue(seed=5)
     want = _single(ens)
     choice = batching.autotune(ens, sample_tiles=4, repeats=1)
-    assert choice["ctas_per_sm"] in (1, 2, 3)
+    assert set(choice["ctas_per_sm"]) == set(batching.METHODS)
+    assert all(k in (1, 2, 3) for k in choice["ctas_per_sm"].values())
     assert all(e.frames_per_chunk in batching.FRAME_CHUNKS for e in ens)
     q = batching.BatchQueue(ens, ctas_per_sm=choice["ctas_per_sm"])
     q.capture()

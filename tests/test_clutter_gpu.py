@@ -212,25 +212,28 @@ def test_filtered_pipeline_matches_fp64_oracle():
     assert rel_l2(host.numpy().reshape(6, 10, 5), expected) < 1e-4
 
 
-@pytest.mark.parametrize("storage,precision,domain", [("float32", "complex128", "beamformed"),
-                                                      ("bf16x2", "bf16x3", "beamformed"),
-                                                      ("bf16x2", "bf16x3", "channel")])
-def test_host_sequence_matches_single_runs(storage, precision, domain):
+@pytest.mark.parametrize("storage,precision,domain,deterministic", [("float32", "complex128", "beamformed", False),
+                                                                    ("bf16x2", "bf16x3", "beamformed", False),
+                                                                    ("bf16x2", "bf16x3", "beamformed", True),
+                                                                    ("bf16x2", "bf16x3", "channel", False)])
+def test_host_sequence_matches_single_runs(storage, precision, domain, deterministic):
     """run_host_sequence (uploads overlapping the previous ensemble's reconstruction) returns, for
     three different ensembles in a row, the powers of separate runs.  The SIMT path is deterministic;
-    the tensor-core DAS starts each item's channel walk where the other CTAs are, so its float32 sums
-    run in a timing-dependent order (~1e-7 of the IQ), which removing the 100x stronger tissue
-    signal amplifies in the filtered power: 5e-5, under the 1e-4 bar of the filtered pipeline."""
+    by default the tensor-core DAS starts each item's channel walk where the other CTAs are, so its
+    float32 sums run in a timing-dependent order (~1e-7 of the IQ), which removing the 100x stronger
+    tissue signal amplifies in the filtered power: 5e-5, under the 1e-4 bar of the filtered pipeline.
+    With ``deterministic=True`` every tile walks its channels in one order and the DAS is
+    bit-identical; what remains is the float64 atomic order of the Gram (1e-12)."""
     scenes = [_scene(seed=s) for s in (5, 6, 7)]
     _, _, angles, t0, grid, geom = scenes[0]
     plan = pipeline.FilteredOpw(scenes[0][0].shape, angles, t0, grid, geom, rank_start=3, precision=precision,
-                                iq_storage=storage, domain=domain)
+                                iq_storage=storage, domain=domain, deterministic=deterministic)
     single = [plan.run(_dev(rc), _dev(cr)).cpu().numpy().ravel() for rc, cr, *_ in scenes]
     pairs = [(torch.from_numpy(rc).pin_memory(), torch.from_numpy(cr).pin_memory()) for rc, cr, *_ in scenes]
     outs = plan.run_host_sequence(pairs)
     plan.check()
     assert len(outs) == 3
-    tol = 1e-12 if storage == "float32" else 5e-5
+    tol = 1e-12 if storage == "float32" else (1e-10 if deterministic else 5e-5)
     for got, want in zip(outs, single):
         assert rel_l2(got.numpy(), want) <= tol
     with pytest.raises(ValueError, match="one output"):
@@ -282,3 +285,37 @@ def test_projection_rows_match_float64(rows, nt, k, mode, offset):
     if out is not None:
         np.testing.assert_allclose(out.cpu().numpy().reshape(rows, nt), resid, rtol=0,
                                    atol=2e-6 * np.abs(resid).max() + 1e-6)
+
+
+@pytest.mark.parametrize("rows,nt,k", [(1, 8, 1), (1000, 64, 3), (20001, 200, 4), (333, 400, 2)])
+def test_refine_vectors_is_float64_gram_product(rows, nt, k):
+    """rcabeam_refine_vectors_device adds X^H (X V) in float64 (complex64 rows)."""
+    rng = np.random.default_rng(rows + k)
+    host = (rng.normal(size=(rows, nt)) + 1j * rng.normal(size=(rows, nt))).astype(np.complex64)
+    v = rng.normal(size=(nt, k)) + 1j * rng.normal(size=(nt, k))
+    z = torch.zeros(k * nt, dtype=torch.complex128, device="cuda")
+    _lib.call("rcabeam_refine_vectors_device", _dev(host).data_ptr(), rows, nt,
+              _dev(np.ravel(v, order="F")).data_ptr(), k, z.data_ptr())
+    x = host.astype(np.complex128)
+    want = x.conj().T @ (x @ v)
+    got = z.cpu().numpy().reshape(k, nt).T
+    np.testing.assert_allclose(got, want, rtol=1e-11, atol=1e-11 * np.abs(want).max())
+
+
+def test_refined_basis_is_closer_to_float64():
+    """One float64 subspace step brings the 3xBF16 Gram's leading vectors to the float64 span."""
+    gen = torch.Generator(device="cuda").manual_seed(4)
+    from rcabeam_b200 import scenes
+
+    iq = scenes.clutter_casorati(200_000, 64, generator=gen, device="cuda")
+    _, b64 = gpu_clutter.temporal_basis(iq)
+    _, b16 = gpu_clutter.temporal_basis(iq, precision="bf16x3")
+    lead64, lead16 = b64[:, :3], b16[:, :3].contiguous()
+    z = torch.zeros(3 * 64, dtype=torch.complex128, device="cuda")
+    _lib.call("rcabeam_refine_vectors_device", iq.data_ptr(), iq.shape[0], 64,
+              lead16.transpose(0, 1).contiguous().data_ptr(), 3, z.data_ptr())
+    q, _ = torch.linalg.qr(z.view(3, 64).transpose(0, 1))
+    p64 = lead64 @ lead64.conj().T
+    before = torch.linalg.matrix_norm(lead16 @ lead16.conj().T - p64).item()
+    after = torch.linalg.matrix_norm(q @ q.conj().T - p64).item()
+    assert after < before
