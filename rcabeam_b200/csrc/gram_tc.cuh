@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc(const __grid_constant__ C
   }
 }
 
-// 3xBF16 Gram with the converters loading rows straight from global memory.
+// Tensor-core Gram with the converters loading rows straight from global memory.
 // gram_tc<false> stages every float32 row block in shared memory by TMA and
 // the converters read it back before writing the BF16 hi / lo operands: per
 // 16-row stage that is 48 KB written + 48 KB read on top of the 48 KB of
@@ -347,8 +347,10 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc(const __grid_constant__ C
 // shared-memory bandwidth, not the tensor pipe.  Here seven converter warps
 // (every warp but the MMA warp) load their 8-column pieces with 16-byte global
 // loads one stage ahead in registers, split them and store only the operands
-// (a 3-stage operand ring).  Same units, operand layout, MMAs and epilogue as
-// gram_tc<false>, so the same sums in the same order.
+// (a 3-stage operand ring).  Same units, operand layouts, MMAs and epilogue as
+// gram_tc, so the same sums in the same order.  TF32 operands (rounded to
+// nearest) are written in the layout the TMA's 32-byte-granule 128-byte swizzle
+// gives gram_tc<true>.
 constexpr int kDirectRing = 3;
 constexpr int kDirectWarps = 7;
 constexpr int kDirectConverters = kDirectWarps * 32;
@@ -358,7 +360,8 @@ __host__ __device__ inline size_t direct_smem_bytes(int nload_max) {
   return size_t(kDirectRing) * nload_max * kSlotBytes + 1024 + 1024;
 }
 
-__global__ void __launch_bounds__(kThreads, 1) gram_bf16_direct(const float* __restrict__ y, const Params p) {
+template <bool TF32>
+__global__ void __launch_bounds__(kThreads, 1) gram_direct(const float* __restrict__ y, const Params p) {
   using namespace rcb::tc;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -410,7 +413,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_bf16_direct(const float* __r
   if (warp == 1) {
     // ------------------------------------------------------------------ MMA --
     if (lane == 0) {
-      const uint32_t idesc = idesc_mn(false, 128, 128);
+      const uint32_t idesc = idesc_mn(TF32, 128, 128);
       int flushes = 0;
       for (int k = 0; k < nstages; ++k) {
         const int s_ = k % kDirectRing;
@@ -419,15 +422,25 @@ __global__ void __launch_bounds__(kThreads, 1) gram_bf16_direct(const float* __r
         if (!mbar_wait(&op_full[s_], (k / kDirectRing) & 1, p.err, kErrWaitFull)) break;
         tc_fence_after();
         const uint32_t op = smem_u32(operands + s_ * stage_bytes);
-        const uint32_t hi = op, lo = op + uint32_t(p.nload_max) * (kSlotBytes / 2);
         for (int t = 0; t < u.ntask; ++t) {
           const uint32_t d = tmem + uint32_t(kBlock * t);
-          const uint32_t ah = hi + u.a_slot[t] * (kSlotBytes / 2), al = lo + u.a_slot[t] * (kSlotBytes / 2);
-          const uint32_t bh = hi + u.b_slot[t] * (kSlotBytes / 2), bl = lo + u.b_slot[t] * (kSlotBytes / 2);
-          mma_f16(d, smem_desc(ah, 2048, 1024, kLayoutSw128), smem_desc(bh, 2048, 1024, kLayoutSw128), idesc,
-                  in_seg > 0 ? 1u : 0u);
-          mma_f16(d, smem_desc(al, 2048, 1024, kLayoutSw128), smem_desc(bh, 2048, 1024, kLayoutSw128), idesc, 1u);
-          mma_f16(d, smem_desc(ah, 2048, 1024, kLayoutSw128), smem_desc(bl, 2048, 1024, kLayoutSw128), idesc, 1u);
+          if constexpr (TF32) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+              const uint32_t a = op + u.a_slot[t] * kSlotBytes + q * 1024;
+              const uint32_t b = op + u.b_slot[t] * kSlotBytes + q * 1024;
+              mma_tf32(d, smem_desc(a, 2048, 512, kLayoutSw128Base32), smem_desc(b, 2048, 512, kLayoutSw128Base32),
+                       idesc, (in_seg > 0 || q > 0) ? 1u : 0u);
+            }
+          } else {
+            const uint32_t hi = op, lo = op + uint32_t(p.nload_max) * (kSlotBytes / 2);
+            const uint32_t ah = hi + u.a_slot[t] * (kSlotBytes / 2), al = lo + u.a_slot[t] * (kSlotBytes / 2);
+            const uint32_t bh = hi + u.b_slot[t] * (kSlotBytes / 2), bl = lo + u.b_slot[t] * (kSlotBytes / 2);
+            mma_f16(d, smem_desc(ah, 2048, 1024, kLayoutSw128), smem_desc(bh, 2048, 1024, kLayoutSw128), idesc,
+                    in_seg > 0 ? 1u : 0u);
+            mma_f16(d, smem_desc(al, 2048, 1024, kLayoutSw128), smem_desc(bh, 2048, 1024, kLayoutSw128), idesc, 1u);
+            mma_f16(d, smem_desc(ah, 2048, 1024, kLayoutSw128), smem_desc(bl, 2048, 1024, kLayoutSw128), idesc, 1u);
+          }
         }
         mma_commit(&op_empty[s_]);
         if (in_seg == kStagesPerFlush - 1 || k == nstages - 1) {
@@ -457,9 +470,11 @@ __global__ void __launch_bounds__(kThreads, 1) gram_bf16_direct(const float* __r
         buf[j][1] = buf[j][0];
         if (i < items) {
           const int slot = i >> 8, rem = i & 255;
-          const int row = rem >> 4, atom = (rem >> 3) & 1, c = rem & 7;
+          const int row = rem >> 4;
+          // 8 columns: BF16 (64-column atom, 8-column chunk) or TF32 (32-column box, 32-byte granule).
+          const int piece = TF32 ? (((rem >> 2) & 3) * 32 + (rem & 3) * 8) : (((rem >> 3) & 1) * 64 + (rem & 7) * 8);
           const long long r = rbase + row;
-          const long long col = (long long)u.load[slot] * kBlock + atom * 64 + c * 8;
+          const long long col = (long long)u.load[slot] * kBlock + piece;
           if (r < r1 && col < cols) {
             const float4* src = reinterpret_cast<const float4*>(y + r * cols + col);
             buf[j][0] = __ldg(src);
@@ -482,16 +497,30 @@ __global__ void __launch_bounds__(kThreads, 1) gram_bf16_direct(const float* __r
         const int i = ct + j * kDirectConverters;
         if (i < items) {
           const int slot = i >> 8, rem = i & 255;
-          const int row = rem >> 4, atom = (rem >> 3) & 1, c = rem & 7;
-          const int sw = row & 7;
+          const int row = rem >> 4;
           const float4 x0 = cur[j][0], x1 = cur[j][1];
-          const float v[8] = {x0.x * prescale, x0.y * prescale, x0.z * prescale, x0.w * prescale,
-                              x1.x * prescale, x1.y * prescale, x1.z * prescale, x1.w * prescale};
-          uint4 h, l;
-          split8(v, h, l);
-          const int off = slot * (kSlotBytes / 2) + atom * 2048 + (row >> 3) * 1024 + sw * 128 + ((c ^ sw) << 4);
-          *reinterpret_cast<uint4*>(hi + off) = h;
-          *reinterpret_cast<uint4*>(lo + off) = l;
+          if constexpr (TF32) {
+            // MN-major 128-byte swizzle with 32-byte granules: 32-column boxes of 16 rows x 128 B,
+            // granule g of row r at (g ^ (r & 3)) x 32 B (4-row atoms, SBO = 512 B).
+            const int box = (rem >> 2) & 3, g = rem & 3;
+            const int off = slot * kSlotBytes + box * 2048 + row * 128 + ((g ^ (row & 3)) << 5);
+            const float4 a = make_float4(round_tf32(x0.x * prescale), round_tf32(x0.y * prescale),
+                                         round_tf32(x0.z * prescale), round_tf32(x0.w * prescale));
+            const float4 b = make_float4(round_tf32(x1.x * prescale), round_tf32(x1.y * prescale),
+                                         round_tf32(x1.z * prescale), round_tf32(x1.w * prescale));
+            *reinterpret_cast<float4*>(hi + off) = a;
+            *reinterpret_cast<float4*>(hi + off + 16) = b;
+          } else {
+            const int atom = (rem >> 3) & 1, c = rem & 7;
+            const int sw = row & 7;
+            const float v[8] = {x0.x * prescale, x0.y * prescale, x0.z * prescale, x0.w * prescale,
+                                x1.x * prescale, x1.y * prescale, x1.z * prescale, x1.w * prescale};
+            uint4 h, l;
+            split8(v, h, l);
+            const int off = slot * (kSlotBytes / 2) + atom * 2048 + (row >> 3) * 1024 + sw * 128 + ((c ^ sw) << 4);
+            *reinterpret_cast<uint4*>(hi + off) = h;
+            *reinterpret_cast<uint4*>(lo + off) = l;
+          }
         }
       }
       fence_async_smem();  // generic-proxy writes -> visible to the tensor core

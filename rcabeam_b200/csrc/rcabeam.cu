@@ -768,10 +768,12 @@ rcabeam_status rcabeam_clutter_scale_device(const void* iq, size_t n, int comple
 // Tensor-core Gram (precision 2 = TF32, 3 = 3xBF16) of a complex64 Casorati
 // matrix: the rows x 2T float32 view as a 2-D tensor with 32 x 16 SWIZZLE_128B
 // boxes, one CTA per (unit, row slice).
-// RCABEAM_GRAM_KERNEL=staged selects the TMA-staged 3xBF16 Gram (a/b timing).
-static bool gram_staged_bf16() {
+// Direct-load Gram for 3xBF16 unless RCABEAM_GRAM_KERNEL=staged; for TF32 only with
+// RCABEAM_GRAM_KERNEL=direct (a/b timing while its operand layout is being checked).
+static bool gram_direct(bool tf32) {
   const char* v = std::getenv("RCABEAM_GRAM_KERNEL");
-  return v && std::string(v) == "staged";
+  const std::string kind = v ? v : "";
+  return tf32 ? kind == "direct" : kind != "staged";
 }
 
 static rcabeam_status gram_tc_launch(const void* iq, size_t rows, size_t nt, const double* scale, bool tf32,
@@ -803,10 +805,10 @@ static rcabeam_status gram_tc_launch(const void* iq, size_t rows, size_t nt, con
          CU_TENSOR_MAP_INTERLEAVE_NONE, tf32 ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B : CU_TENSOR_MAP_SWIZZLE_128B,
          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return RCABEAM_ERROR_ARGUMENT;
-  if (!tf32 && !gram_staged_bf16()) {
-    // 3xBF16: converters load the rows from global memory (no TMA staging).
+  if (gram_direct(tf32)) {
+    // Converters load the rows from global memory (no TMA staging).
     const size_t smem = std::max(gramtc::direct_smem_bytes(prm.nload_max), size_t(120) << 10);
-    auto kern = gramtc::gram_bf16_direct;
+    auto kern = tf32 ? gramtc::gram_direct<true> : gramtc::gram_direct<false>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
       return RCABEAM_ERROR_CUDA;
     kern<<<unsigned(prm.nunits * prm.slices), gramtc::kThreads, smem>>>(static_cast<const float*>(iq), prm);
