@@ -162,10 +162,11 @@ rcabeam_status rcabeam_pack_ensemble_split_device(const void* source, void* hi, 
  * over 64-voxel tiles).  precision bit 0 clear: rc_hi / cr_hi are FP16-packed
  * channels (rcabeam_pack_ensemble_fp16_device), rc_lo / cr_lo unused; bit 0
  * set: BF16 hi / lo planes from rcabeam_pack_ensemble_split_device.  Bit 1 set:
- * every tile walks its channels in one fixed order, so repeated calls give
- * bit-identical results (clear: each tile starts where the other SMs are,
- * which keeps their sample windows in L2 together but makes the order of the
- * float32 sums, and their last bits, depend on timing).  Coefficients are
+ * every tile starts its channel walk at the same slot (clear: each tile starts
+ * where the other SMs are, which keeps their sample windows in L2 together but
+ * makes the order of the float32 sums depend on timing); the interleaving of
+ * the builder warps still varies, so repeated calls agree to about 1e-7 of the
+ * IQ instead of being bit-identical.  Coefficients are
  * split into hi + lo halves; accumulation is float32.  pd, signal and
  * geometry_workspace are as for rcabeam_ensemble_device (method 0).  Requires
  * nt % 4 == 0 and 16-byte aligned planes (RCABEAM_ERROR_ARGUMENT otherwise).
@@ -214,13 +215,13 @@ rcabeam_status rcabeam_heevd_device(double* gram, double* eigenvalues, size_t nt
 rcabeam_status rcabeam_project_device(const void* iq, void* out, double* power, size_t rows, size_t nt,
                                       int complex128, const double* vectors, size_t k, int mode);
 
-/* One float64 subspace-iteration step (complex64 rows): z (device, column-major
- * nt x k complex128, zeroed by the caller) += X^H (X V) for the k <= 4
- * column-major (nt x k) complex128 vectors V, nt <= 512.  Orthonormalizing z
+/* One float64 subspace-iteration step on complex64 rows X (extension): the k <= 4
+ * column-major (nt x k, nt <= 512) complex128 vectors V are replaced, in place,
+ * by an orthonormal basis (float64 modified Gram-Schmidt) of X^H (X V).  This
  * refines dominant Gram eigenvectors from a reduced-precision Gram against the
- * exact float64 Gram, without forming it. */
-rcabeam_status rcabeam_refine_vectors_device(const void* iq, size_t rows, size_t nt, const double* vectors,
-                                             size_t k, double* z);
+ * exact float64 Gram without forming it.  z: caller scratch of nt x k complex128. */
+rcabeam_status rcabeam_refine_vectors_device(const void* iq, size_t rows, size_t nt, double* vectors, size_t k,
+                                             double* z);
 
 /* Bytes of geometry_workspace that rcabeam_ensemble_device / rcabeam_opw_fp16_device
  * actually use for nv voxels (at most the documented 2*nv*(nc+na) float4).  A

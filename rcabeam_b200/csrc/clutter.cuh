@@ -595,5 +595,62 @@ __global__ void __launch_bounds__(kRefineThreads)
   }
 }
 
+// Orthonormal basis of the k <= kRefineMax vectors z (row c = vector c, nt <= 512
+// complex128) into out: modified Gram-Schmidt in float64, each projection
+// applied twice (re-orthogonalization), one CTA of kRefineThreads threads.
+__device__ __forceinline__ double2 block_sum2(double2 v, double2* red) {
+  for (int off = 16; off > 0; off >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();  // previous use of red is complete
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double2 t = make_double2(0.0, 0.0);
+  for (int w = 0; w < int(blockDim.x >> 5); ++w) {
+    t.x += red[w].x;
+    t.y += red[w].y;
+  }
+  return t;
+}
+
+__global__ void __launch_bounds__(kRefineThreads) orthonormalize(const double2* __restrict__ z, double2* __restrict__ out,
+                                                                 int nt, int k) {
+  __shared__ double2 v[kRefineMax][512];
+  __shared__ double2 red[kRefineThreads / 32];
+  for (int i = threadIdx.x; i < k * nt; i += blockDim.x) v[i / nt][i % nt] = z[i];
+  __syncthreads();
+  for (int c = 0; c < k; ++c) {
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int j = 0; j < c; ++j) {
+        double2 d = make_double2(0.0, 0.0);  // <v_j, v_c> = sum conj(v_j) v_c
+        for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+          const double2 a = v[j][t], b = v[c][t];
+          d.x = fma(a.x, b.x, fma(a.y, b.y, d.x));
+          d.y = fma(a.x, b.y, fma(-a.y, b.x, d.y));
+        }
+        d = block_sum2(d, red);
+        for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+          const double2 a = v[j][t];
+          v[c][t].x -= d.x * a.x - d.y * a.y;
+          v[c][t].y -= d.x * a.y + d.y * a.x;
+        }
+        __syncthreads();
+      }
+    }
+    double2 n = make_double2(0.0, 0.0);
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) n.x = fma(v[c][t].x, v[c][t].x, fma(v[c][t].y, v[c][t].y, n.x));
+    n = block_sum2(n, red);
+    const double inv = n.x > 0.0 ? 1.0 / sqrt(n.x) : 0.0;
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+      v[c][t].x *= inv;
+      v[c][t].y *= inv;
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < k * nt; i += blockDim.x) out[i] = v[i / nt][i % nt];
+}
+
 }  // namespace clutter
 }  // namespace rcb

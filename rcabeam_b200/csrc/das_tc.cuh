@@ -112,7 +112,8 @@ struct Args {
   int ncols;       // 2 * frames
   int nbox;        // TMA boxes per plane of a full pass (the stage layout)
   int ntiles;
-  int walk_fixed;  // 1: every item walks the channel slots from slot 0 (run-to-run identical sums)
+  int walk_fixed;  // 1: every item walks the channel slots from slot 0 (no timing-dependent start)
+  int seg_steps;   // MMA steps between accumulator flushes (float32 accumulation length)
   int* err;
 };
 
@@ -671,7 +672,7 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
         issued = true;
         mma_commit(&empty[s]);  // frees the stage once these MMAs have read it
         ++k;
-        if (++seg == kSegSteps) flush(kAccPartial);
+        if (++seg == p.seg_steps) flush(kAccPartial);
       }
       // Every issued MMA has completed before the warp leaves (TMEM is freed after).
       mma_commit(drain);

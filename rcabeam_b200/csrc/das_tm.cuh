@@ -459,7 +459,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         issued = true;
         tc::mma_commit(&empty_x[sx]);
         tc::mma_commit(&empty_a[sa]);
-        if (++seg == kSegSteps) flush(tc::kAccPartial);
+        if (++seg == p.seg_steps) flush(tc::kAccPartial);
       }
       tc::mma_commit(drain);
       mbar_wait(drain, 0, p.err, kErrWaitDrain);

@@ -372,15 +372,23 @@ static rcabeam_status run_tm(tc::Args a) {
   return launch_status();
 }
 
-// Which tensor-core OPW kernel runs: the TMEM-coefficient kernel unless
-// RCABEAM_DAS_KERNEL=smem selects the shared-memory-coefficient one (a/b timing).
+// Which tensor-core OPW kernel runs: the shared-memory-coefficient kernel unless
+// RCABEAM_DAS_KERNEL=tmem selects the TMEM-coefficient one (a/b timing).
 static bool use_tm_kernel() {
   const char* v = std::getenv("RCABEAM_DAS_KERNEL");
-  return !(v && std::string(v) == "smem");
+  return v && std::string(v) == "tmem";
+}
+
+// MMA steps per float32 accumulation segment (RCABEAM_TC_SEGMENT overrides, for a/b runs).
+static int segment_steps() {
+  const char* v = std::getenv("RCABEAM_TC_SEGMENT");
+  const int n = v ? std::atoi(v) : 0;
+  return n >= 16 && n <= 4096 ? n : tc::kSegSteps;
 }
 
 template <bool BF16X3>
 static rcabeam_status run_tc(tc::Args a) {
+  a.seg_steps = segment_steps();
   if (use_tm_kernel()) return run_tm<BF16X3>(a);
   const size_t nt = size_t(a.nt);
   // The deepest ring (one builder warp per stage) that fits shared memory.
@@ -904,11 +912,12 @@ rcabeam_status rcabeam_project_device(const void* iq, void* out, double* power, 
   return launch_status();
 }
 
-rcabeam_status rcabeam_refine_vectors_device(const void* iq, size_t rows, size_t nt, const double* vectors,
-                                             size_t k, double* z) {
+rcabeam_status rcabeam_refine_vectors_device(const void* iq, size_t rows, size_t nt, double* vectors, size_t k,
+                                             double* z) {
   if (!iq || !vectors || !z || !rows || !nt || nt > 512 || !k || k > size_t(clutter::kRefineMax) ||
       reinterpret_cast<uintptr_t>(iq) % 8 != 0)
     return RCABEAM_ERROR_ARGUMENT;
+  if (cudaMemsetAsync(z, 0, nt * k * 2 * sizeof(double), 0) != cudaSuccess) return RCABEAM_ERROR_CUDA;
   const size_t smem = size_t(clutter::kRefineMax) * nt * 16 + size_t(clutter::kRefineRows) * clutter::kRefineMax * 16 +
                       size_t(clutter::kRefineRows) * nt * 8;
   if (cudaFuncSetAttribute(clutter::refine_vectors, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) !=
@@ -920,6 +929,8 @@ rcabeam_status rcabeam_refine_vectors_device(const void* iq, size_t rows, size_t
   const size_t blocks = std::min<size_t>(size_t(sms) * 4, (rows + clutter::kRefineRows - 1) / clutter::kRefineRows);
   clutter::refine_vectors<<<unsigned(blocks), clutter::kRefineThreads, smem>>>(
       static_cast<const float2*>(iq), rows, int(nt), reinterpret_cast<const double2*>(vectors), int(k), z);
+  clutter::orthonormalize<<<1, clutter::kRefineThreads>>>(reinterpret_cast<const double2*>(z),
+                                                          reinterpret_cast<double2*>(vectors), int(nt), int(k));
   return launch_status();
 }
 

@@ -222,8 +222,8 @@ def test_host_sequence_matches_single_runs(storage, precision, domain, determini
     by default the tensor-core DAS starts each item's channel walk where the other CTAs are, so its
     float32 sums run in a timing-dependent order (~1e-7 of the IQ), which removing the 100x stronger
     tissue signal amplifies in the filtered power: 5e-5, under the 1e-4 bar of the filtered pipeline.
-    With ``deterministic=True`` every tile walks its channels in one order and the DAS is
-    bit-identical; what remains is the float64 atomic order of the Gram (1e-12)."""
+    With ``deterministic=True`` every tile walks its channels from the same slot, so only the
+    interleaving of the builder warps' steps stays timing dependent: 2e-6, 25x below."""
     scenes = [_scene(seed=s) for s in (5, 6, 7)]
     _, _, angles, t0, grid, geom = scenes[0]
     plan = pipeline.FilteredOpw(scenes[0][0].shape, angles, t0, grid, geom, rank_start=3, precision=precision,
@@ -233,7 +233,7 @@ def test_host_sequence_matches_single_runs(storage, precision, domain, determini
     outs = plan.run_host_sequence(pairs)
     plan.check()
     assert len(outs) == 3
-    tol = 1e-12 if storage == "float32" else (1e-10 if deterministic else 5e-5)
+    tol = 1e-12 if storage == "float32" else (1e-5 if deterministic else 5e-5)
     for got, want in zip(outs, single):
         assert rel_l2(got.numpy(), want) <= tol
     with pytest.raises(ValueError, match="one output"):
@@ -263,6 +263,8 @@ def test_projection_rows_match_float64(rows, nt, k, mode, offset):
     """rcabeam_project_device on complex64 rows (the streamed kernel for even frame counts and
     16-byte aligned rows; the warp-per-row kernel for odd counts or an 8-byte offset) against
     float64 NumPy: power to 1e-12 relative, written rows to float32 rounding."""
+    if k > nt:
+        pytest.skip("k temporal vectors need k <= nt frames")
     rng = np.random.default_rng(rows + nt + k)
     host = (rng.normal(size=(rows, nt)) + 1j * rng.normal(size=(rows, nt))).astype(np.complex64)
     host[:, :] += 50 * np.exp(2j * np.pi * 0.01 * np.arange(nt))  # a strong common component
@@ -281,25 +283,28 @@ def test_projection_rows_match_float64(rows, nt, k, mode, offset):
     resid = x - part if mode & 1 else part
     want = (np.sum(np.abs(resid) ** 2, axis=1) if mode & 1 else np.sum(np.abs(y) ** 2, axis=1)) / nt
     got = power.cpu().numpy()
-    np.testing.assert_allclose(got, want, rtol=1e-11, atol=1e-12 * want.max())
+    scale = np.mean(np.abs(x) ** 2)  # a residual can be exactly zero (k = nt): rounding is relative to |x|^2
+    np.testing.assert_allclose(got, want, rtol=1e-11, atol=1e-12 * max(want.max(), scale))
     if out is not None:
         np.testing.assert_allclose(out.cpu().numpy().reshape(rows, nt), resid, rtol=0,
                                    atol=2e-6 * np.abs(resid).max() + 1e-6)
 
 
 @pytest.mark.parametrize("rows,nt,k", [(1, 8, 1), (1000, 64, 3), (20001, 200, 4), (333, 400, 2)])
-def test_refine_vectors_is_float64_gram_product(rows, nt, k):
-    """rcabeam_refine_vectors_device adds X^H (X V) in float64 (complex64 rows)."""
+def test_refine_vectors_is_float64_subspace_step(rows, nt, k):
+    """rcabeam_refine_vectors_device replaces V by an orthonormal basis of X^H (X V) (float64)."""
     rng = np.random.default_rng(rows + k)
     host = (rng.normal(size=(rows, nt)) + 1j * rng.normal(size=(rows, nt))).astype(np.complex64)
     v = rng.normal(size=(nt, k)) + 1j * rng.normal(size=(nt, k))
-    z = torch.zeros(k * nt, dtype=torch.complex128, device="cuda")
-    _lib.call("rcabeam_refine_vectors_device", _dev(host).data_ptr(), rows, nt,
-              _dev(np.ravel(v, order="F")).data_ptr(), k, z.data_ptr())
+    iq = _dev(host)
+    vec = _dev(np.ravel(v, order="F"))
+    z = torch.empty(k * nt, dtype=torch.complex128, device="cuda")
+    _lib.call("rcabeam_refine_vectors_device", iq.data_ptr(), rows, nt, vec.data_ptr(), k, z.data_ptr())
     x = host.astype(np.complex128)
-    want = x.conj().T @ (x @ v)
-    got = z.cpu().numpy().reshape(k, nt).T
-    np.testing.assert_allclose(got, want, rtol=1e-11, atol=1e-11 * np.abs(want).max())
+    q, _ = np.linalg.qr(x.conj().T @ (x @ v))
+    got = vec.cpu().numpy().reshape(k, nt).T
+    np.testing.assert_allclose(got.conj().T @ got, np.eye(k), atol=1e-12)
+    np.testing.assert_allclose(got @ got.conj().T, q @ q.conj().T, atol=1e-10)
 
 
 def test_refined_basis_is_closer_to_float64():
@@ -310,12 +315,12 @@ def test_refined_basis_is_closer_to_float64():
     iq = scenes.clutter_casorati(200_000, 64, generator=gen, device="cuda")
     _, b64 = gpu_clutter.temporal_basis(iq)
     _, b16 = gpu_clutter.temporal_basis(iq, precision="bf16x3")
-    lead64, lead16 = b64[:, :3], b16[:, :3].contiguous()
-    z = torch.zeros(3 * 64, dtype=torch.complex128, device="cuda")
-    _lib.call("rcabeam_refine_vectors_device", iq.data_ptr(), iq.shape[0], 64,
-              lead16.transpose(0, 1).contiguous().data_ptr(), 3, z.data_ptr())
-    q, _ = torch.linalg.qr(z.view(3, 64).transpose(0, 1))
+    lead64 = b64[:, :3]
+    rows = b16[:, :3].transpose(0, 1).contiguous()  # (3, 64): vector c in row c
+    before = rows.transpose(0, 1).clone()
+    z = torch.empty(3 * 64, dtype=torch.complex128, device="cuda")
+    _lib.call("rcabeam_refine_vectors_device", iq.data_ptr(), iq.shape[0], 64, rows.data_ptr(), 3, z.data_ptr())
+    after = rows.transpose(0, 1)
     p64 = lead64 @ lead64.conj().T
-    before = torch.linalg.matrix_norm(lead16 @ lead16.conj().T - p64).item()
-    after = torch.linalg.matrix_norm(q @ q.conj().T - p64).item()
-    assert after < before
+    err = lambda b: torch.linalg.matrix_norm(b @ b.conj().T - p64).item()  # noqa: E731
+    assert err(after) < err(before)
