@@ -417,7 +417,13 @@ static rcabeam_status run_tc(tc::Args a) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  auto kern = stages == 6 ? tc::opw_tc<BF16X3, 6>
+  // Seven builder warps over the six-stage ring when RCABEAM_TC_BUILDERS=7 (a/b runs;
+  // 12 warps = 3 per SM sub-partition, so the 168-register budget still fits).
+  const char* nb = std::getenv("RCABEAM_TC_BUILDERS");
+  const bool seven = stages == 6 && nb && std::atoi(nb) == 7;
+  const int builders = seven ? 7 : stages;
+  auto kern = seven         ? tc::opw_tc<BF16X3, 6, 7>
+              : stages == 6 ? tc::opw_tc<BF16X3, 6>
               : stages == 5 ? tc::opw_tc<BF16X3, 5>
               : stages == 4 ? tc::opw_tc<BF16X3, 4>
               : stages == 3 ? tc::opw_tc<BF16X3, 3>
@@ -429,7 +435,7 @@ static rcabeam_status run_tc(tc::Args a) {
   if (!a.partial || !a.slot_clock) return RCABEAM_ERROR_CUDA;
   const int items = a.ntiles * a.chunks;
   const unsigned grid = unsigned(std::min(std::min(items, sms), tc::kMaxCtas));
-  kern<<<grid, tc::threads_for(stages), smem>>>(mh[0], mh[1], ml[0], ml[1], a);
+  kern<<<grid, tc::threads_for(builders), smem>>>(mh[0], mh[1], ml[0], ml[1], a);
   return launch_status();
 }
 
