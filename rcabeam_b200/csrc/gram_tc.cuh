@@ -73,6 +73,7 @@ struct Unit {
 
 struct Params {
   int nunits, slices, nload_max, nt;
+  int tf32_swizzle;  // direct TF32 operand layout: granule ^= (row & 3) (0) or ((row >> 1) & 3) (1)
   long long rows, slice_rows;
   const double* scale;
   double* upper;
@@ -503,7 +504,8 @@ __global__ void __launch_bounds__(kThreads, 1) gram_direct(const float* __restri
             // MN-major 128-byte swizzle with 32-byte granules: 32-column boxes of 16 rows x 128 B,
             // granule g of row r at (g ^ (r & 3)) x 32 B (4-row atoms, SBO = 512 B).
             const int box = (rem >> 2) & 3, g = rem & 3;
-            const int off = slot * kSlotBytes + box * 2048 + row * 128 + ((g ^ (row & 3)) << 5);
+            const int sw = p.tf32_swizzle ? ((row >> 1) & 3) : (row & 3);
+            const int off = slot * kSlotBytes + box * 2048 + row * 128 + ((g ^ sw) << 5);
             const float4 a = make_float4(round_tf32(x0.x * prescale), round_tf32(x0.y * prescale),
                                          round_tf32(x0.z * prescale), round_tf32(x0.w * prescale));
             const float4 b = make_float4(round_tf32(x1.x * prescale), round_tf32(x1.y * prescale),

@@ -787,7 +787,7 @@ rcabeam_status rcabeam_clutter_scale_device(const void* iq, size_t n, int comple
 static bool gram_direct(bool tf32) {
   const char* v = std::getenv("RCABEAM_GRAM_KERNEL");
   const std::string kind = v ? v : "";
-  return tf32 ? kind == "direct" : kind != "staged";
+  return tf32 ? (kind == "direct" || kind == "direct2") : kind != "staged";
 }
 
 static rcabeam_status gram_tc_launch(const void* iq, size_t rows, size_t nt, const double* scale, bool tf32,
@@ -819,6 +819,10 @@ static rcabeam_status gram_tc_launch(const void* iq, size_t rows, size_t nt, con
          CU_TENSOR_MAP_INTERLEAVE_NONE, tf32 ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B : CU_TENSOR_MAP_SWIZZLE_128B,
          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return RCABEAM_ERROR_ARGUMENT;
+  {
+    const char* v = std::getenv("RCABEAM_GRAM_KERNEL");
+    prm.tf32_swizzle = v && std::string(v) == "direct2" ? 1 : 0;
+  }
   if (gram_direct(tf32)) {
     // Converters load the rows from global memory (no TMA staging).
     const size_t smem = std::max(gramtc::direct_smem_bytes(prm.nload_max), size_t(120) << 10);
