@@ -359,7 +359,6 @@ __global__ void __launch_bounds__(128)
 // different order (float64 rounding differences only).  Every wait is bounded.
 constexpr int kPipeConsumers = 8;
 constexpr int kPipeStages = 3;
-constexpr int kPipeMaxFrames = 32;  // frames per lane: G * 32 >= nt
 
 template <int G>
 struct PipeShape {
@@ -380,8 +379,10 @@ struct PipeShape {
   }
 };
 
-template <int G>
-__global__ void __launch_bounds__(PipeShape<G>::kThreads, 1)
+// MAXF frames per lane (G * MAXF >= nt); MAXF = 16 keeps the registers low enough for
+// two CTAs (sixteen consumer warps) per SM.
+template <int G, int MAXF>
+__global__ void __launch_bounds__(PipeShape<G>::kThreads, MAXF <= 16 ? 2 : 1)
     project_rows_pipe(const float2* __restrict__ x, float2* __restrict__ out, double* __restrict__ power,
                       size_t rows, int nt, const double2* __restrict__ vec, int k, int mode, double inv_nt,
                       int* err) {
@@ -433,9 +434,9 @@ __global__ void __launch_bounds__(PipeShape<G>::kThreads, 1)
     const size_t r0 = b * S::kRows;
     const bool valid = r0 + rs < rows;
     const float2* xr = reinterpret_cast<const float2*>(ring + size_t(s) * stage_bytes + size_t(rs) * stride);
-    float2 xv[kPipeMaxFrames];
+    float2 xv[MAXF];
 #pragma unroll
-    for (int m = 0; m < kPipeMaxFrames; ++m) {
+    for (int m = 0; m < MAXF; ++m) {
       const int t = j + G * m;
       xv[m] = t < nt ? xr[t] : make_float2(0.f, 0.f);
     }
@@ -445,7 +446,7 @@ __global__ void __launch_bounds__(PipeShape<G>::kThreads, 1)
 #pragma unroll
     for (int c = 0; c < kProjSmall; ++c) yr[c] = yi[c] = 0.0;
 #pragma unroll
-    for (int m = 0; m < kPipeMaxFrames; ++m) {
+    for (int m = 0; m < MAXF; ++m) {
       const int t = j + G * m;
       if (t < nt) {
         const double ar = double(xv[m].x), ai = double(xv[m].y);
@@ -475,7 +476,7 @@ __global__ void __launch_bounds__(PipeShape<G>::kThreads, 1)
     if (mode & 3) {
       float2* orow = (mode & 2) ? out + (r0 + rs) * size_t(nt) : nullptr;
 #pragma unroll
-      for (int m = 0; m < kPipeMaxFrames; ++m) {
+      for (int m = 0; m < MAXF; ++m) {
         const int t = j + G * m;
         if (t < nt) {
           double px = 0.0, py = 0.0;

@@ -608,11 +608,11 @@ static void launch_project(const void* iq, void* out, double* power, size_t rows
 
 // Streamed projection (complex64 rows, k <= 4, even nt <= 512, 16-byte aligned
 // rows): one CTA per SM, G lanes per row.  False when the form does not apply.
-template <int G>
+template <int G, int MAXF>
 static bool launch_project_pipe(const void* iq, void* out, double* power, size_t rows, size_t nt,
                                 const double* vec, size_t k, int mode) {
   using S = clutter::PipeShape<G>;
-  auto kern = clutter::project_rows_pipe<G>;
+  auto kern = clutter::project_rows_pipe<G, MAXF>;
   const size_t smem = S::smem_bytes(int(nt));
   if (smem > 227 * 1024 ||
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
@@ -621,7 +621,8 @@ static bool launch_project_pipe(const void* iq, void* out, double* power, size_t
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const size_t blocks = (rows + S::kRows - 1) / S::kRows;
-  const unsigned grid = unsigned(std::min<size_t>(blocks, size_t(sms)));
+  const size_t per_sm = (MAXF <= 16 && 2 * smem <= 227 * 1024) ? 2 : 1;
+  const unsigned grid = unsigned(std::min<size_t>(blocks, per_sm * size_t(sms)));
   kern<<<grid, S::kThreads, smem>>>(static_cast<const float2*>(iq), static_cast<float2*>(out), power, rows, int(nt),
                                     reinterpret_cast<const double2*>(vec), int(k), mode, 1.0 / double(nt),
                                     device_error_ptr());
@@ -633,9 +634,9 @@ static bool project_pipe(const void* iq, void* out, double* power, size_t rows, 
   if (k > size_t(clutter::kProjSmall) || nt % 2 || nt > 512 || reinterpret_cast<uintptr_t>(iq) % 16 != 0 ||
       rows > (size_t(1) << 40))
     return false;
-  if (nt <= 128) return launch_project_pipe<4>(iq, out, power, rows, nt, vec, k, mode);
-  if (nt <= 256) return launch_project_pipe<8>(iq, out, power, rows, nt, vec, k, mode);
-  return launch_project_pipe<16>(iq, out, power, rows, nt, vec, k, mode);
+  // 16 lanes per row, 2 rows per warp, 16-row stages.
+  if (nt <= 256) return launch_project_pipe<16, 16>(iq, out, power, rows, nt, vec, k, mode);
+  return launch_project_pipe<16, 32>(iq, out, power, rows, nt, vec, k, mode);
 }
 
 template <typename IN>

@@ -37,9 +37,9 @@ _CHANNEL_STAGES = ("gram", "eig", "filter", "pack", "das")
 class FilteredOpw:
     """Fixed-shape filtered-OPW pipeline: ``run(rc, cr) -> (nx, nz, ny)`` float64 filtered power.
 
-    At a tensor-core Gram precision (``"tf32"``, ``"bf16x3"``) the discarded leading
-    vectors get one float64 subspace-iteration step against the exact Gram
-    (``refine``, default on when the smaller projector is ranks [0, rank_start)).
+    ``refine=True`` gives the discarded leading vectors of a tensor-core Gram
+    (``"tf32"``, ``"bf16x3"``) one float64 subspace-iteration step against the
+    exact Gram (when the smaller projector is ranks [0, rank_start)).
     ``iq_storage="bf16x2"`` runs the tensor-core DAS on split-BF16 planes; with
     ``deterministic=True`` every tile starts its channel walk at the same slot
     (by default each tile starts where the other SMs are, which keeps their
@@ -49,7 +49,7 @@ class FilteredOpw:
 
     def __init__(self, channel_shape, angles, t_start, grid, geom: RCAGeometry, *, rank_start: int = 3,
                  rank_stop: int | None = None, precision: str = "complex128", iq_storage: str = "float32",
-                 group=None, domain: str = "beamformed", deterministic: bool = False, refine: bool | None = None):
+                 group=None, domain: str = "beamformed", deterministic: bool = False, refine: bool = False):
         ns, nc, na, nt = (int(n) for n in channel_shape)
         self.shape = (len(grid[0]), len(grid[1]), len(grid[2]))
         self.channel_shape = (ns, nc, na, nt)
@@ -101,11 +101,11 @@ class FilteredOpw:
         self.subtract = stop - start > nt - (stop - start)
         self.k = (start + nt - stop) if self.subtract else (stop - start)
         self.vectors = torch.empty((max(self.k, 1), nt), dtype=torch.complex128, device=dev)
-        # Float64 subspace refinement of the discarded leading vectors (one X^H (X V) pass)
-        # when the Gram runs at a tensor-core precision; only when the smaller projector is
-        # the leading ranks [0, rank_start) (subtract mode, rank_stop = nt).
+        # Optional float64 subspace refinement of the discarded leading vectors (one X^H (X V)
+        # pass) for tensor-core Gram precisions; only when the smaller projector is the
+        # leading ranks [0, rank_start) (subtract mode, rank_stop = nt).
         leading = self.subtract and stop == nt and 0 < self.k <= 4
-        self.refine = (precision in ("tf32", "bf16x3") if refine is None else bool(refine)) and leading
+        self.refine = bool(refine) and leading
         if self.refine and (domain != "beamformed" or group is not None):
             self.refine = False
         self.refined = torch.empty((max(self.k, 1), nt), dtype=torch.complex128, device=dev)
