@@ -215,13 +215,13 @@ rcabeam_status rcabeam_heevd_device(double* gram, double* eigenvalues, size_t nt
 rcabeam_status rcabeam_project_device(const void* iq, void* out, double* power, size_t rows, size_t nt,
                                       int complex128, const double* vectors, size_t k, int mode);
 
-/* One float64 subspace-iteration step on complex64 rows X (extension): the k <= 4
- * column-major (nt x k, nt <= 512) complex128 vectors V are replaced, in place,
- * by an orthonormal basis (float64 modified Gram-Schmidt) of X^H (X V).  This
- * refines dominant Gram eigenvectors from a reduced-precision Gram against the
- * exact float64 Gram without forming it.  z: caller scratch of nt x k complex128. */
-rcabeam_status rcabeam_refine_vectors_device(const void* iq, size_t rows, size_t nt, double* vectors, size_t k,
-                                             double* z);
+/* Float64 Rayleigh-Ritz matrix on complex64 rows X (extension): h (device,
+ * m x m complex128, column-major; cleared inside) = (X V)^H (X V) for the m <= 16
+ * vectors V (m x nt row-major complex128, vector c in row c, nt <= 512), i.e.
+ * V^H (X^H X) V without forming the Gram.  Its eigenvectors rotate V onto the
+ * float64 Gram's eigenvectors within span(V). */
+rcabeam_status rcabeam_ritz_matrix_device(const void* iq, size_t rows, size_t nt, const double* vectors, size_t m,
+                                         double* h);
 
 /* Bytes of geometry_workspace that rcabeam_ensemble_device / rcabeam_opw_fp16_device
  * actually use for nv voxels (at most the documented 2*nv*(nc+na) float4).  A

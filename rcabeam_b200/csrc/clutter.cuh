@@ -505,152 +505,65 @@ __global__ void __launch_bounds__(PipeShape<G>::kThreads, MAXF <= 16 ? 2 : 1)
   }
 }
 
-// One float64 subspace-iteration step for the dominant temporal vectors:
-// z += X^H (X V) over rows [r0, r1) of the Casorati matrix, V = nt x k
-// (column-major complex128, k <= kRefineMax), z = nt x k (column-major
-// complex128, accumulated with atomics).  The Gram of the tensor-core
-// precisions is rounded to 16-bit / TF32 operands; multiplying the current
-// vectors by the exact float64 Gram (without forming it) and re-orthonormalizing
-// shrinks their error by the gap ratio lambda_{k+1} / lambda_k.
-// Per CTA: blocks of kRefineRows rows are staged in shared memory (complex64);
-// each warp forms y = x V for two rows (float64 dot products, warp
-// reductions), then every thread accumulates conj(x_t) y_c for its frames t.
-constexpr int kRefineMax = 4;
-constexpr int kRefineRows = 16;
-constexpr int kRefineThreads = 256;
+constexpr int kRefineRows = 16;  // Casorati rows staged per block of the Rayleigh-Ritz pass
 
-__global__ void __launch_bounds__(kRefineThreads)
-    refine_vectors(const float2* __restrict__ x, size_t rows, int nt, const double2* __restrict__ vec, int k,
-                   double* __restrict__ z) {
+// Float64 Rayleigh-Ritz matrix of the Casorati rows on m <= kRitzMax vectors:
+// h (m x m complex128, column-major, accumulated with atomics) += Y^H Y with
+// Y = X V, i.e. V^H G V for the exact Gram G = X^H X, without forming G.  Per
+// CTA, blocks of kRefineRows rows are staged in shared memory; thread (row, c)
+// forms y[row][c] over all frames, then thread (i, j) accumulates
+// conj(y[r][i]) y[r][j] over the block's rows in a register.  V's rows are
+// staged with a padded stride so that the 16 vectors a warp reads sit in
+// distinct banks.
+constexpr int kRitzMax = 16;
+constexpr int kRitzThreads = kRefineRows * kRitzMax;  // 256
+
+__host__ __device__ inline int ritz_stride(int nt) { return nt + 1; }  // double2 elements per staged vector
+
+__global__ void __launch_bounds__(kRitzThreads)
+    ritz_matrix(const float2* __restrict__ x, size_t rows, int nt, const double2* __restrict__ vec, int m,
+                double* __restrict__ h) {
   extern __shared__ __align__(16) unsigned char smem[];
-  double2* vs = reinterpret_cast<double2*>(smem);                 // [k][nt]
-  double2* ys = vs + size_t(kRefineMax) * nt;                     // [rows][k]
-  float2* xs = reinterpret_cast<float2*>(ys + kRefineRows * kRefineMax);  // [rows][nt]
-  for (int i = threadIdx.x; i < k * nt; i += blockDim.x) vs[i] = vec[i];
+  const int vs_stride = ritz_stride(nt);
+  double2* vs = reinterpret_cast<double2*>(smem);                        // [m][nt + 1]
+  double2* ys = vs + size_t(kRitzMax) * vs_stride;                       // [rows][kRitzMax]
+  float2* xs = reinterpret_cast<float2*>(ys + kRefineRows * kRitzMax);   // [rows][nt]
+  for (int i = threadIdx.x; i < m * nt; i += blockDim.x) vs[(i / nt) * vs_stride + i % nt] = vec[i];
   const size_t per = (rows + gridDim.x - 1) / gridDim.x;
   const size_t r0 = size_t(blockIdx.x) * per, r1 = min(rows, r0 + per);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  constexpr int kFramesPerThread = 2;  // nt <= 512 = 2 x 256
-  double zr[kFramesPerThread][kRefineMax], zi[kFramesPerThread][kRefineMax];
-#pragma unroll
-  for (int f = 0; f < kFramesPerThread; ++f)
-#pragma unroll
-    for (int c = 0; c < kRefineMax; ++c) zr[f][c] = zi[f][c] = 0.0;
+  const int pr = threadIdx.x / kRitzMax, pc = threadIdx.x % kRitzMax;  // (row, vector) of phase 1
+  const int hi = threadIdx.x / kRitzMax, hj = threadIdx.x % kRitzMax;  // (i, j) of phase 2
+  double hr = 0.0, him = 0.0;
   for (size_t b = r0; b < r1; b += kRefineRows) {
     const int nr = int(min(size_t(kRefineRows), r1 - b));
-    __syncthreads();  // the previous block's rows and coordinates are no longer read
+    __syncthreads();
     for (int i = threadIdx.x; i < nr * nt; i += blockDim.x) xs[i] = x[b * size_t(nt) + i];
     __syncthreads();
-    // Coordinates y[r][c] = sum_t x[r][t] v_c[t] (two rows per warp).
-    for (int rr = 2 * warp; rr < 2 * warp + 2; ++rr) {
-      for (int c = 0; c < k; ++c) {
-        double yr = 0.0, yi = 0.0;
-        if (rr < nr) {
-          for (int t = lane; t < nt; t += 32) {
-            const float2 a = xs[rr * nt + t];
-            const double2 v = vs[c * nt + t];
-            yr = fma(double(a.x), v.x, fma(-double(a.y), v.y, yr));
-            yi = fma(double(a.x), v.y, fma(double(a.y), v.x, yi));
-          }
-        }
-        for (int off = 16; off > 0; off >>= 1) {
-          yr += __shfl_xor_sync(0xffffffffu, yr, off);
-          yi += __shfl_xor_sync(0xffffffffu, yi, off);
-        }
-        if (lane == 0) ys[rr * kRefineMax + c] = make_double2(rr < nr ? yr : 0.0, rr < nr ? yi : 0.0);
+    double yr = 0.0, yi = 0.0;
+    if (pr < nr && pc < m) {
+      const float2* xr = xs + pr * nt;
+      const double2* vr = vs + pc * vs_stride;
+      for (int t = 0; t < nt; ++t) {
+        const float2 a = xr[t];
+        const double2 v = vr[t];
+        yr = fma(double(a.x), v.x, fma(-double(a.y), v.y, yr));
+        yi = fma(double(a.x), v.y, fma(double(a.y), v.x, yi));
       }
     }
+    ys[pr * kRitzMax + pc] = make_double2(yr, yi);
     __syncthreads();
-    // z[t][c] += conj(x[r][t]) y[r][c].
-#pragma unroll
-    for (int f = 0; f < kFramesPerThread; ++f) {
-      const int t = threadIdx.x + f * kRefineThreads;
-      if (t < nt) {
-        for (int r = 0; r < nr; ++r) {
-          const float2 a = xs[r * nt + t];
-          const double ar = double(a.x), ai = double(a.y);
-#pragma unroll
-          for (int c = 0; c < kRefineMax; ++c) {
-            if (c < k) {
-              const double2 y = ys[r * kRefineMax + c];
-              zr[f][c] = fma(ar, y.x, fma(ai, y.y, zr[f][c]));
-              zi[f][c] = fma(ar, y.y, fma(-ai, y.x, zi[f][c]));
-            }
-          }
-        }
+    if (hi < m && hj < m) {
+      for (int r = 0; r < nr; ++r) {
+        const double2 a = ys[r * kRitzMax + hi], c = ys[r * kRitzMax + hj];
+        hr = fma(a.x, c.x, fma(a.y, c.y, hr));   // conj(a) c
+        him = fma(a.x, c.y, fma(-a.y, c.x, him));
       }
     }
   }
-#pragma unroll
-  for (int f = 0; f < kFramesPerThread; ++f) {
-    const int t = threadIdx.x + f * kRefineThreads;
-    if (t < nt) {
-#pragma unroll
-      for (int c = 0; c < kRefineMax; ++c) {
-        if (c < k) {
-          atomicAdd(z + 2 * (size_t(c) * nt + t), zr[f][c]);
-          atomicAdd(z + 2 * (size_t(c) * nt + t) + 1, zi[f][c]);
-        }
-      }
-    }
+  if (hi < m && hj < m) {
+    atomicAdd(h + 2 * (size_t(hj) * m + hi), hr);  // column-major (i, j)
+    atomicAdd(h + 2 * (size_t(hj) * m + hi) + 1, him);
   }
-}
-
-// Orthonormal basis of the k <= kRefineMax vectors z (row c = vector c, nt <= 512
-// complex128) into out: modified Gram-Schmidt in float64, each projection
-// applied twice (re-orthogonalization), one CTA of kRefineThreads threads.
-__device__ __forceinline__ double2 block_sum2(double2 v, double2* red) {
-  for (int off = 16; off > 0; off >>= 1) {
-    v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
-    v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
-  }
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __syncthreads();  // previous use of red is complete
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  double2 t = make_double2(0.0, 0.0);
-  for (int w = 0; w < int(blockDim.x >> 5); ++w) {
-    t.x += red[w].x;
-    t.y += red[w].y;
-  }
-  return t;
-}
-
-__global__ void __launch_bounds__(kRefineThreads) orthonormalize(const double2* __restrict__ z, double2* __restrict__ out,
-                                                                 int nt, int k) {
-  __shared__ double2 v[kRefineMax][512];
-  __shared__ double2 red[kRefineThreads / 32];
-  for (int i = threadIdx.x; i < k * nt; i += blockDim.x) v[i / nt][i % nt] = z[i];
-  __syncthreads();
-  for (int c = 0; c < k; ++c) {
-    for (int pass = 0; pass < 2; ++pass) {
-      for (int j = 0; j < c; ++j) {
-        double2 d = make_double2(0.0, 0.0);  // <v_j, v_c> = sum conj(v_j) v_c
-        for (int t = threadIdx.x; t < nt; t += blockDim.x) {
-          const double2 a = v[j][t], b = v[c][t];
-          d.x = fma(a.x, b.x, fma(a.y, b.y, d.x));
-          d.y = fma(a.x, b.y, fma(-a.y, b.x, d.y));
-        }
-        d = block_sum2(d, red);
-        for (int t = threadIdx.x; t < nt; t += blockDim.x) {
-          const double2 a = v[j][t];
-          v[c][t].x -= d.x * a.x - d.y * a.y;
-          v[c][t].y -= d.x * a.y + d.y * a.x;
-        }
-        __syncthreads();
-      }
-    }
-    double2 n = make_double2(0.0, 0.0);
-    for (int t = threadIdx.x; t < nt; t += blockDim.x) n.x = fma(v[c][t].x, v[c][t].x, fma(v[c][t].y, v[c][t].y, n.x));
-    n = block_sum2(n, red);
-    const double inv = n.x > 0.0 ? 1.0 / sqrt(n.x) : 0.0;
-    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
-      v[c][t].x *= inv;
-      v[c][t].y *= inv;
-    }
-    __syncthreads();
-  }
-  for (int i = threadIdx.x; i < k * nt; i += blockDim.x) out[i] = v[i / nt][i % nt];
 }
 
 }  // namespace clutter

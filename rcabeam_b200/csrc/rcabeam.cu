@@ -923,25 +923,23 @@ rcabeam_status rcabeam_project_device(const void* iq, void* out, double* power, 
   return launch_status();
 }
 
-rcabeam_status rcabeam_refine_vectors_device(const void* iq, size_t rows, size_t nt, double* vectors, size_t k,
-                                             double* z) {
-  if (!iq || !vectors || !z || !rows || !nt || nt > 512 || !k || k > size_t(clutter::kRefineMax) ||
+rcabeam_status rcabeam_ritz_matrix_device(const void* iq, size_t rows, size_t nt, const double* vectors, size_t m,
+                                         double* h) {
+  if (!iq || !vectors || !h || !rows || !nt || nt > 512 || !m || m > size_t(clutter::kRitzMax) ||
       reinterpret_cast<uintptr_t>(iq) % 8 != 0)
     return RCABEAM_ERROR_ARGUMENT;
-  if (cudaMemsetAsync(z, 0, nt * k * 2 * sizeof(double), 0) != cudaSuccess) return RCABEAM_ERROR_CUDA;
-  const size_t smem = size_t(clutter::kRefineMax) * nt * 16 + size_t(clutter::kRefineRows) * clutter::kRefineMax * 16 +
-                      size_t(clutter::kRefineRows) * nt * 8;
-  if (cudaFuncSetAttribute(clutter::refine_vectors, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) !=
+  if (cudaMemsetAsync(h, 0, m * m * 2 * sizeof(double), 0) != cudaSuccess) return RCABEAM_ERROR_CUDA;
+  const size_t smem = size_t(clutter::kRitzMax) * clutter::ritz_stride(int(nt)) * 16 +
+                      size_t(clutter::kRefineRows) * clutter::kRitzMax * 16 + size_t(clutter::kRefineRows) * nt * 8;
+  if (cudaFuncSetAttribute(clutter::ritz_matrix, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) !=
       cudaSuccess)
     return RCABEAM_ERROR_CUDA;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const size_t blocks = std::min<size_t>(size_t(sms) * 4, (rows + clutter::kRefineRows - 1) / clutter::kRefineRows);
-  clutter::refine_vectors<<<unsigned(blocks), clutter::kRefineThreads, smem>>>(
-      static_cast<const float2*>(iq), rows, int(nt), reinterpret_cast<const double2*>(vectors), int(k), z);
-  clutter::orthonormalize<<<1, clutter::kRefineThreads>>>(reinterpret_cast<const double2*>(z),
-                                                          reinterpret_cast<double2*>(vectors), int(nt), int(k));
+  const size_t blocks = std::min<size_t>(size_t(sms) * 3, (rows + clutter::kRefineRows - 1) / clutter::kRefineRows);
+  clutter::ritz_matrix<<<unsigned(blocks), clutter::kRitzThreads, smem>>>(
+      static_cast<const float2*>(iq), rows, int(nt), reinterpret_cast<const double2*>(vectors), int(m), h);
   return launch_status();
 }
 

@@ -37,9 +37,10 @@ _CHANNEL_STAGES = ("gram", "eig", "filter", "pack", "das")
 class FilteredOpw:
     """Fixed-shape filtered-OPW pipeline: ``run(rc, cr) -> (nx, nz, ny)`` float64 filtered power.
 
-    ``refine=True`` gives the discarded leading vectors of a tensor-core Gram
-    (``"tf32"``, ``"bf16x3"``) one float64 subspace-iteration step against the
-    exact Gram (when the smaller projector is ranks [0, rank_start)).
+    ``refine=True`` corrects the discarded leading vectors of a tensor-core Gram
+    (``"tf32"``, ``"bf16x3"``) by a float64 Rayleigh-Ritz step on its 16 leading
+    eigenvectors against the exact Gram (one extra pass over the IQ; when the
+    smaller projector is ranks [0, rank_start)).
     ``iq_storage="bf16x2"`` runs the tensor-core DAS on split-BF16 planes; with
     ``deterministic=True`` every tile starts its channel walk at the same slot
     (by default each tile starts where the other SMs are, which keeps their
@@ -101,14 +102,17 @@ class FilteredOpw:
         self.subtract = stop - start > nt - (stop - start)
         self.k = (start + nt - stop) if self.subtract else (stop - start)
         self.vectors = torch.empty((max(self.k, 1), nt), dtype=torch.complex128, device=dev)
-        # Optional float64 subspace refinement of the discarded leading vectors (one X^H (X V)
-        # pass) for tensor-core Gram precisions; only when the smaller projector is the
-        # leading ranks [0, rank_start) (subtract mode, rank_stop = nt).
+        # Optional float64 Rayleigh-Ritz correction of the discarded leading vectors (one pass
+        # over the IQ) for tensor-core Gram precisions; only when the smaller projector is
+        # the leading ranks [0, rank_start) (subtract mode, rank_stop = nt).
         leading = self.subtract and stop == nt and 0 < self.k <= 4
         self.refine = bool(refine) and leading
         if self.refine and (domain != "beamformed" or group is not None):
             self.refine = False
-        self.refined = torch.empty((max(self.k, 1), nt), dtype=torch.complex128, device=dev)
+        # Rayleigh-Ritz subspace: the m leading eigenvectors (m = k + 13, at most 16 and T).
+        self.ritz_m = min(nt, self.k + 13, 16)
+        self.ritz_basis = torch.empty((self.ritz_m, nt), dtype=torch.complex128, device=dev)
+        self.ritz = Gram(self.ritz_m, dev) if self.refine else None
         self.events = [torch.cuda.Event(enable_timing=True) for _ in range(len(_STAGES) + 1)]
         self.last_das_event_ms = None
 
@@ -123,9 +127,17 @@ class FilteredOpw:
             torch.index_select(vt, 0, ranks, out=self.vectors[: self.k])
 
     def _refine(self) -> None:
-        """One float64 subspace-iteration step: vectors <- orthonormal basis of X^H (X V) (no host sync)."""
-        _lib.call("rcabeam_refine_vectors_device", self.iq.data_ptr(), self.nv, self.channel_shape[3],
-                  self.vectors.data_ptr(), self.k, self.refined.data_ptr())
+        """Float64 Rayleigh-Ritz on the m leading eigenvectors of the reduced-precision Gram:
+        H = (X V_m)^H (X V_m) in float64 (one pass over the IQ), H's eigenvectors rotate V_m,
+        and the k with the largest Ritz values replace the discarded vectors (no host sync)."""
+        nt, m, k = self.channel_shape[3], self.ritz_m, self.k
+        vt = torch.view_as_complex(self.gram.matrix.view(nt, nt, 2))  # row e: e-th eigenvector (ascending)
+        torch.index_select(vt, 0, torch.arange(nt - 1, nt - 1 - m, -1, device=self.device), out=self.ritz_basis)
+        _lib.call("rcabeam_ritz_matrix_device", self.iq.data_ptr(), self.nv, nt, self.ritz_basis.data_ptr(), m,
+                  self.ritz.matrix.data_ptr())
+        self.ritz.decompose()  # ascending Ritz values; row c of the view = c-th Ritz vector's coefficients
+        u = torch.view_as_complex(self.ritz.matrix.view(m, m, 2))[m - k:].flip(0)  # k largest, descending
+        torch.matmul(u, self.ritz_basis, out=self.vectors[:k])
 
     def run(self, rc: torch.Tensor, cr: torch.Tensor, after_inputs=None) -> torch.Tensor:
         """Filtered power of resident complex64 RC/CR channels ``(ns, nc, na, nt)``.
@@ -299,7 +311,7 @@ class FilteredOpw:
         das = 1 if self.storage != "float32" and self.channel_shape[3] % 4 == 0 else 2
         if self.domain == "channel":  # scale x2, Gram x2, finish, projection x2, pack x2, order, DAS
             return 5 + 2 + 2 + 6 + das
-        return 2 + 6 + das + 4 + (2 if self.refine else 0)
+        return 2 + 6 + das + 4 + (1 if self.refine else 0)
 
 
 def synthetic_channels(shape, *, generator: torch.Generator, device, scale: float = 1.0):

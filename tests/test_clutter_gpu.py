@@ -290,37 +290,37 @@ def test_projection_rows_match_float64(rows, nt, k, mode, offset):
                                    atol=2e-6 * np.abs(resid).max() + 1e-6)
 
 
-@pytest.mark.parametrize("rows,nt,k", [(1, 8, 1), (1000, 64, 3), (20001, 200, 4), (333, 400, 2)])
-def test_refine_vectors_is_float64_subspace_step(rows, nt, k):
-    """rcabeam_refine_vectors_device replaces V by an orthonormal basis of X^H (X V) (float64)."""
-    rng = np.random.default_rng(rows + k)
+@pytest.mark.parametrize("rows,nt,m", [(1, 8, 1), (1000, 64, 16), (20001, 200, 16), (333, 400, 5)])
+def test_ritz_matrix_is_float64_projected_gram(rows, nt, m):
+    """rcabeam_ritz_matrix_device forms (X V)^H (X V) in float64 (complex64 rows, column-major)."""
+    rng = np.random.default_rng(rows + m)
     host = (rng.normal(size=(rows, nt)) + 1j * rng.normal(size=(rows, nt))).astype(np.complex64)
-    v = rng.normal(size=(nt, k)) + 1j * rng.normal(size=(nt, k))
-    iq = _dev(host)
-    vec = _dev(np.ravel(v, order="F"))
-    z = torch.empty(k * nt, dtype=torch.complex128, device="cuda")
-    _lib.call("rcabeam_refine_vectors_device", iq.data_ptr(), rows, nt, vec.data_ptr(), k, z.data_ptr())
-    x = host.astype(np.complex128)
-    q, _ = np.linalg.qr(x.conj().T @ (x @ v))
-    got = vec.cpu().numpy().reshape(k, nt).T
-    np.testing.assert_allclose(got.conj().T @ got, np.eye(k), atol=1e-12)
-    np.testing.assert_allclose(got @ got.conj().T, q @ q.conj().T, atol=1e-10)
+    v = rng.normal(size=(m, nt)) + 1j * rng.normal(size=(m, nt))  # vector c in row c
+    iq, vec = _dev(host), _dev(v)
+    h = torch.empty(m * m, dtype=torch.complex128, device="cuda")
+    _lib.call("rcabeam_ritz_matrix_device", iq.data_ptr(), rows, nt, vec.data_ptr(), m, h.data_ptr())
+    y = host.astype(np.complex128) @ v.T
+    want = y.conj().T @ y
+    got = h.cpu().numpy().reshape(m, m).T  # column-major storage
+    np.testing.assert_allclose(got, want, rtol=1e-11, atol=1e-11 * np.abs(want).max())
 
 
-def test_refined_basis_is_closer_to_float64():
-    """One float64 subspace step brings the 3xBF16 Gram's leading vectors to the float64 span."""
+def test_ritz_refinement_recovers_float64_leading_span():
+    """FilteredOpw's Rayleigh-Ritz step on the 3xBF16 Gram's leading vectors lands on the float64
+    Gram's leading span (the scene model has a rank-3 tissue band)."""
     gen = torch.Generator(device="cuda").manual_seed(4)
     from rcabeam_b200 import scenes
 
     iq = scenes.clutter_casorati(200_000, 64, generator=gen, device="cuda")
     _, b64 = gpu_clutter.temporal_basis(iq)
     _, b16 = gpu_clutter.temporal_basis(iq, precision="bf16x3")
-    lead64 = b64[:, :3]
-    rows = b16[:, :3].transpose(0, 1).contiguous()  # (3, 64): vector c in row c
-    before = rows.transpose(0, 1).clone()
-    z = torch.empty(3 * 64, dtype=torch.complex128, device="cuda")
-    _lib.call("rcabeam_refine_vectors_device", iq.data_ptr(), iq.shape[0], 64, rows.data_ptr(), 3, z.data_ptr())
-    after = rows.transpose(0, 1)
-    p64 = lead64 @ lead64.conj().T
+    p64 = b64[:, :3] @ b64[:, :3].conj().T
+    m = 16
+    basis = b16[:, :m].transpose(0, 1).contiguous()
+    h = gpu_clutter.Gram(m, iq.device)
+    _lib.call("rcabeam_ritz_matrix_device", iq.data_ptr(), iq.shape[0], 64, basis.data_ptr(), m, h.matrix.data_ptr())
+    h.decompose()
+    u = torch.view_as_complex(h.matrix.view(m, m, 2))[m - 3:]
+    refined = (u @ basis).transpose(0, 1)
     err = lambda b: torch.linalg.matrix_norm(b @ b.conj().T - p64).item()  # noqa: E731
-    assert err(after) < err(before)
+    assert err(refined) < 1e-3 * err(b16[:, :3]) + 1e-12

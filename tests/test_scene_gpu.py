@@ -103,22 +103,25 @@ def test_config1_scene_split_inside_the_noise_band():
     ranks, whose eigenvalues lie within a few percent of each other: the per-voxel filtered
     power then moves to first order with any rotation of the Gram inside that band.  Forms
     with a float64 Gram stay within 1e-4 of the float64 chain; the 3xBF16 Gram's rounding
-    rotates the split by ~1e-4 (printed, bounded at 2e-4), which the plain form's float64
-    Gram on the same split-BF16 DAS removes."""
+    rotates the split by ~1e-4 (printed, bounded at 2e-4), which a float64 Gram on the same
+    split-BF16 DAS, or the float64 Rayleigh-Ritz correction (``refine=True``), removes."""
     scene = scenes.config1_scene(seed=11)
     rc_h, cr_h = scene.rc.cpu().numpy(), scene.cr.cpu().numpy()
     want, _ = _oracle_chain(rc_h, cr_h, scene, 3)
     got = {}
-    for storage, precision in (("float32", "complex128"), ("bf16x2", "complex128"), ("bf16x2", "bf16x3")):
+    for storage, precision, refine in (("float32", "complex128", False), ("bf16x2", "complex128", False),
+                                       ("bf16x2", "bf16x3", False), ("bf16x2", "bf16x3", True)):
         plan = pipeline.FilteredOpw(tuple(scene.rc.shape), scene.angles, scene.t_start, scene.grid, scene.geom,
-                                    rank_start=3, precision=precision, iq_storage=storage)
-        got[(storage, precision)] = rel_l2(plan.run(scene.rc, scene.cr).cpu().numpy().ravel(), want)
+                                    rank_start=3, precision=precision, iq_storage=storage, refine=refine)
+        got[(storage, precision, refine)] = rel_l2(plan.run(scene.rc, scene.cr).cpu().numpy().ravel(), want)
         plan.check()
-        print(f"config 1, rank_start 3: DAS {storage:8s} Gram {precision:10s} filtered PD rel L2 "
-              f"{got[(storage, precision)]:.3e}")
-    assert got[("float32", "complex128")] <= 1e-4
-    assert got[("bf16x2", "complex128")] <= 1e-4
-    assert got[("bf16x2", "bf16x3")] <= 2e-4
+        print(f"config 1, rank_start 3: DAS {storage:8s} Gram {precision:10s} refine {int(refine)} "
+              f"filtered PD rel L2 {got[(storage, precision, refine)]:.3e}")
+    assert got[("float32", "complex128", False)] <= 1e-4
+    assert got[("bf16x2", "complex128", False)] <= 1e-4
+    assert got[("bf16x2", "bf16x3", False)] <= 2e-4
+    # The float64 Rayleigh-Ritz step on the 16 leading vectors (all 16 frames here) is exact.
+    assert got[("bf16x2", "bf16x3", True)] <= 1e-4
 
 
 def test_config1_scene_fnumber_one():
