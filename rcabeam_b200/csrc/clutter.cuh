@@ -343,168 +343,6 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-// Streamed form of project_rows_one for complex64 rows (k <= kProjSmall, even
-// nt <= 512, 16-byte aligned rows): the same float64 coordinates, residual and
-// power, organized so that HBM reads stay in flight while the float64 work runs.
-//   * one producer warp copies blocks of kRows consecutive rows into a ring of
-//     kPipeStages shared-memory stages with bulk copies (one per row, so each
-//     staged row starts at a bank offset that keeps the consumers' loads
-//     conflict-free);
-//   * kPipeConsumers warps each take kRows / kPipeConsumers rows of a stage,
-//     G lanes per row (frames j, j + G, j + 2G, ... in registers), so the
-//     coordinate reduction is log2(G) shuffle levels inside a lane group;
-//   * the k temporal vectors sit in shared memory, where the lane groups of a
-//     warp read the same frames (broadcast loads).
-// The float64 operation count is that of project_rows_one; the sums run in a
-// different order (float64 rounding differences only).  Every wait is bounded.
-constexpr int kPipeConsumers = 8;
-constexpr int kPipeStages = 3;
-
-template <int G>
-struct PipeShape {
-  static constexpr int kRowsPerWarp = 32 / G;
-  static constexpr int kRows = kPipeConsumers * kRowsPerWarp;  // rows per stage
-  static constexpr int kThreads = (kPipeConsumers + 1) * 32;
-  // Bytes between staged rows: nt * 8 rounded up so that the lane groups of a
-  // half-warp (G lanes x 8 bytes each) start on distinct 8G-byte bank ranges.
-  __host__ __device__ static uint32_t stride(int nt) {
-    uint32_t b = uint32_t(nt) * 8u;
-    const uint32_t want = (8u * G) & 127u;
-    while ((b & 127u) != want) b += 16u;
-    return b;
-  }
-  __host__ __device__ static uint32_t vec_bytes(int nt) { return (uint32_t(kProjSmall) * nt * 16u + 127u) & ~127u; }
-  __host__ __device__ static size_t smem_bytes(int nt) {
-    return 128 + 128 + vec_bytes(nt) + size_t(kPipeStages) * kRows * stride(nt);
-  }
-};
-
-// MAXF frames per lane (G * MAXF >= nt); MAXF = 16 keeps the registers low enough for
-// two CTAs (sixteen consumer warps) per SM.
-template <int G, int MAXF>
-__global__ void __launch_bounds__(PipeShape<G>::kThreads, MAXF <= 16 ? 2 : 1)
-    project_rows_pipe(const float2* __restrict__ x, float2* __restrict__ out, double* __restrict__ power,
-                      size_t rows, int nt, const double2* __restrict__ vec, int k, int mode, double inv_nt,
-                      int* err) {
-  using S = PipeShape<G>;
-  extern __shared__ unsigned char smem_raw[];
-  unsigned char* base =
-      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-  uint64_t* full = reinterpret_cast<uint64_t*>(base);
-  uint64_t* empty = full + kPipeStages;
-  double2* vs = reinterpret_cast<double2*>(base + 128);  // vs[c * nt + t]
-  unsigned char* ring = base + 128 + S::vec_bytes(nt);
-  const uint32_t stride = S::stride(nt);
-  const uint32_t stage_bytes = uint32_t(S::kRows) * stride;
-  const size_t blocks = (rows + S::kRows - 1) / S::kRows;
-  for (int i = threadIdx.x; i < k * nt; i += blockDim.x) vs[i] = vec[i];
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < kPipeStages; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kPipeConsumers);
-    }
-    fence_mbar_init();
-  }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (warp == kPipeConsumers) {
-    // ------------------------------------------------------------ producer --
-    int it = 0;
-    for (size_t b = blockIdx.x; b < blocks; b += gridDim.x, ++it) {
-      const int s = it % kPipeStages;
-      if (!mbar_wait_fast(&empty[s], ((it / kPipeStages) & 1) ^ 1, err, kErrWaitEmpty)) break;
-      const size_t r0 = b * S::kRows;
-      const int n = int(min(size_t(S::kRows), rows - r0));
-      if (lane == 0) mbar_arrive_expect_tx(&full[s], uint32_t(n) * uint32_t(nt) * 8u);
-      __syncwarp();
-      for (int i = lane; i < n; i += 32)
-        bulk_load(ring + size_t(s) * stage_bytes + size_t(i) * stride, x + (r0 + i) * size_t(nt),
-                  uint32_t(nt) * 8u, &full[s]);
-    }
-    return;
-  }
-  // -------------------------------------------------------------- consumers --
-  const int group = lane / G, j = lane % G;
-  const int rs = warp * S::kRowsPerWarp + group;  // row of the stage
-  const bool subtract = mode & 1;
-  int it = 0;
-  for (size_t b = blockIdx.x; b < blocks; b += gridDim.x, ++it) {
-    const int s = it % kPipeStages;
-    if (!mbar_wait_fast(&full[s], (it / kPipeStages) & 1, err, kErrWaitFull)) return;
-    const size_t r0 = b * S::kRows;
-    const bool valid = r0 + rs < rows;
-    const float2* xr = reinterpret_cast<const float2*>(ring + size_t(s) * stage_bytes + size_t(rs) * stride);
-    float2 xv[MAXF];
-#pragma unroll
-    for (int m = 0; m < MAXF; ++m) {
-      const int t = j + G * m;
-      xv[m] = t < nt ? xr[t] : make_float2(0.f, 0.f);
-    }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[s]);  // the row is in registers: the stage may be refilled
-    double yr[kProjSmall], yi[kProjSmall];
-#pragma unroll
-    for (int c = 0; c < kProjSmall; ++c) yr[c] = yi[c] = 0.0;
-#pragma unroll
-    for (int m = 0; m < MAXF; ++m) {
-      const int t = j + G * m;
-      if (t < nt) {
-        const double ar = double(xv[m].x), ai = double(xv[m].y);
-#pragma unroll
-        for (int c = 0; c < kProjSmall; ++c) {
-          if (c < k) {
-            const double2 v = vs[c * nt + t];
-            yr[c] = fma(ar, v.x, fma(-ai, v.y, yr[c]));
-            yi[c] = fma(ar, v.y, fma(ai, v.x, yi[c]));
-          }
-        }
-      }
-    }
-    double retained = 0.0;
-#pragma unroll
-    for (int c = 0; c < kProjSmall; ++c) {
-      if (c < k) {  // k is uniform over the warp
-#pragma unroll
-        for (int off = 1; off < G; off <<= 1) {
-          yr[c] += __shfl_xor_sync(0xffffffffu, yr[c], off);
-          yi[c] += __shfl_xor_sync(0xffffffffu, yi[c], off);
-        }
-        retained += yr[c] * yr[c] + yi[c] * yi[c];
-      }
-    }
-    double pw = 0.0;
-    if (mode & 3) {
-      float2* orow = (mode & 2) ? out + (r0 + rs) * size_t(nt) : nullptr;
-#pragma unroll
-      for (int m = 0; m < MAXF; ++m) {
-        const int t = j + G * m;
-        if (t < nt) {
-          double px = 0.0, py = 0.0;
-#pragma unroll
-          for (int c = 0; c < kProjSmall; ++c) {
-            if (c < k) {  // y * conj(v)
-              const double2 v = vs[c * nt + t];
-              px = fma(yr[c], v.x, fma(yi[c], v.y, px));
-              py = fma(yi[c], v.x, fma(-yr[c], v.y, py));
-            }
-          }
-          const double rx = subtract ? double(xv[m].x) - px : px;
-          const double ry = subtract ? double(xv[m].y) - py : py;
-          pw = fma(rx, rx, fma(ry, ry, pw));
-          if (orow && valid) orow[t] = make_float2(float(rx), float(ry));
-        }
-      }
-    }
-    if (power) {
-      if (subtract) {
-#pragma unroll
-        for (int off = 1; off < G; off <<= 1) pw += __shfl_xor_sync(0xffffffffu, pw, off);
-      }
-      if (j == 0 && valid) power[r0 + rs] = (subtract ? pw : retained) * inv_nt;
-    }
-  }
-}
-
 constexpr int kRefineRows = 16;  // Casorati rows staged per block of the Rayleigh-Ritz pass
 
 // Float64 Rayleigh-Ritz matrix of the Casorati rows on m <= kRitzMax vectors:

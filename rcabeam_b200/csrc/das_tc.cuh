@@ -326,19 +326,14 @@ __device__ __forceinline__ float2 demod_phase(double fd, double tau) {
   return make_float2(cs, sn);
 }
 
-// BUILDERS builder warps over a ring of STAGES stages.  With BUILDERS <= STAGES a
-// builder waits for its stage by mbarrier phase parity, which is unambiguous
-// because at most 2 x STAGES positions are claimed and unconsumed.  With more
-// builders than stages, lane 1 of the MMA warp follows the stages' empty
-// barriers in position order (it can never be two phases behind: a later phase
-// needs a builder it has not released yet) and publishes a monotonic count of
-// consumed positions, on which the builders wait instead.
-template <bool BF16X3, int STAGES, int BUILDERS = STAGES>
-__global__ void __launch_bounds__(threads_for(BUILDERS), 1)
+// One builder warp per ring stage: a builder waits for its stage by mbarrier
+// phase parity, which is unambiguous because no more builders than stages hold
+// claims (at most 2 x STAGES positions are claimed and unconsumed).
+template <bool BF16X3, int STAGES>
+__global__ void __launch_bounds__(threads_for(STAGES), 1)
     opw_tc(const __grid_constant__ CUtensorMap map_rc_hi, const __grid_constant__ CUtensorMap map_cr_hi,
            const __grid_constant__ CUtensorMap map_rc_lo, const __grid_constant__ CUtensorMap map_cr_lo, Args p) {
-  constexpr int kBuilders = BUILDERS;
-  constexpr bool kRelease = BUILDERS > STAGES;
+  constexpr int kBuilders = STAGES;
   constexpr int kMmaWarp = kBuilders;
   using L = Layout<BF16X3>;
   constexpr int kPlanes = L::kPlanes;
@@ -360,8 +355,6 @@ __global__ void __launch_bounds__(threads_for(BUILDERS), 1)
   int* item_steps = counter + 1;                         // steps staged for the current item
   volatile int* acc_kind = item_steps + 1;               // AccKind of the pending flush
   int* walk_start = item_steps + 2;                      // first channel slot of the current item
-  volatile int* released = item_steps + 3;               // positions consumed (kRelease)
-  volatile int* mma_done = item_steps + 4;               // the MMA lane has left its loop
   double* angle_tab = reinterpret_cast<double*>(ctrl + kCtrlBytes);
   // Transmit delay of (aperture, angle, voxel) = tx_base[aperture, angle] (the
   // tile's first voxel, float64) + tx_off (float: within a compact tile the
@@ -381,8 +374,6 @@ __global__ void __launch_bounds__(threads_for(BUILDERS), 1)
     mbar_init(acc_empty, 4);
     mbar_init(drain, 1);
     *counter = 0;
-    *released = 0;
-    *mma_done = 0;
     fence_mbar_init();
   }
   for (int a = threadIdx.x; a < p.na; a += blockDim.x) {
@@ -423,28 +414,8 @@ __global__ void __launch_bounds__(threads_for(BUILDERS), 1)
       uint32_t mine = 0;
       if (lane == 0) mine = uint32_t(atomicAdd(counter, 1));
       k = __shfl_sync(0xffffffffu, mine, 0);
-      if constexpr (kRelease) {
-        // Position k reuses the stage of position k - STAGES: wait until that one is consumed.
-        bool free = true;
-        if (lane == 0 && k >= uint32_t(STAGES)) {
-          const int need = int(k) - STAGES + 1;
-          if (*released < need) {
-            const unsigned long long t0 = global_ns();
-            for (uint32_t i = 0; *released < need; ++i) {
-              if ((i & 255u) == 255u && global_ns() - t0 > kWaitLimitNs) {
-                atomicCAS(p.err, 0, kErrWaitEmpty);
-                free = false;
-                break;
-              }
-            }
-          }
-          __threadfence_block();
-        }
-        return __shfl_sync(0xffffffffu, free, 0);
-      } else {
-        return __all_sync(0xffffffffu,
-                          wait_phase(&empty[k % STAGES], ((k / STAGES) & 1) ^ 1, p.err, kErrWaitEmpty));
-      }
+      return __all_sync(0xffffffffu,
+                        wait_phase(&empty[k % STAGES], ((k / STAGES) & 1) ^ 1, p.err, kErrWaitEmpty));
     };
     // Issues the window copies of a claimed stage before its coefficient rows
     // are written (the copy's latency overlaps the row stores); the warp's 32
@@ -708,27 +679,6 @@ __global__ void __launch_bounds__(threads_for(BUILDERS), 1)
       // Every issued MMA has completed before the warp leaves (TMEM is freed after).
       mma_commit(drain);
       mbar_wait(drain, 0, p.err, kErrWaitDrain);
-      *mma_done = 1;
-    } else if (kRelease && lane == 1) {
-      // Releaser: positions are consumed in order; publish each one's completion.
-      for (uint32_t pos = 0;; ++pos) {
-        bool got = false;
-        const unsigned long long t0 = global_ns();
-        for (uint32_t i = 0;; ++i) {
-          if (mbar_test(&empty[pos % STAGES], (pos / STAGES) & 1)) {
-            got = true;
-            break;
-          }
-          if (*mma_done) break;
-          if ((i & 255u) == 255u && global_ns() - t0 > kWaitLimitNs) {
-            atomicCAS(p.err, 0, kErrWaitEmpty);
-            break;
-          }
-        }
-        if (!got) break;
-        __threadfence_block();
-        *released = int(pos + 1);
-      }
     }
     __syncwarp();
   } else {

@@ -21,7 +21,6 @@
 #include "das_generic.cuh"
 #include "das_staged.cuh"
 #include "das_tc.cuh"
-#include "das_tm.cuh"
 #include "gram_tc.cuh"
 #include "pack.cuh"
 #include "scene.cuh"
@@ -329,56 +328,6 @@ static float2* tc_partials_address() {
   return addresses[dev];
 }
 
-// Frames of the full passes of the TMEM-coefficient kernel (multiple of 8, <= 104).
-static size_t tm_full_frames(size_t nt) {
-  return nt > size_t(tm::kMaxFrames) ? size_t(tm::kMaxFrames) : (nt + 7) / 8 * 8;
-}
-
-// Tensor-core OPW with the coefficients in tensor memory (das_tm.cuh).
-template <bool BF16X3>
-static rcabeam_status run_tm(tc::Args a) {
-  const size_t nt = size_t(a.nt);
-  a.chunks = int((nt + tm::kMaxFrames - 1) / tm::kMaxFrames);
-  const int frames = int(tm_full_frames(nt));
-  a.frames = frames;
-  a.last_frames = int((nt - size_t(frames) * size_t(a.chunks - 1) + 7) / 8 * 8);
-  a.ncols = 2 * frames;
-  a.nbox = (a.ncols + tc::kBoxCols - 1) / tc::kBoxCols;
-  a.ntiles = int((size_t(a.nv) + tc::kVox - 1) / tc::kVox);
-  const size_t smem = tm::Layout<BF16X3>::bytes(a.nbox, a.na) + 1024;
-  if (smem > 227 * 1024) return RCABEAM_ERROR_ARGUMENT;
-  CUtensorMap mh[2], ml[2];
-  const size_t slabs = size_t(a.nc) * a.na;
-  for (int i = 0; i < 2; ++i) {
-    if (!make_plane_map(&mh[i], a.x_hi[i], nt, size_t(a.ns), slabs)) return RCABEAM_ERROR_CUDA;
-    if (BF16X3) {
-      if (!make_plane_map(&ml[i], a.x_lo[i], nt, size_t(a.ns), slabs)) return RCABEAM_ERROR_CUDA;
-    } else {
-      ml[i] = mh[i];
-    }
-  }
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  auto kern = tm::opw_tm<BF16X3>;
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
-    return RCABEAM_ERROR_CUDA;
-  a.partial = tc_partials_address();
-  a.slot_clock = tc_slot_clock_address();
-  if (!a.partial || !a.slot_clock) return RCABEAM_ERROR_CUDA;
-  const int items = a.ntiles * a.chunks;
-  const unsigned grid = unsigned(std::min(std::min(items, sms), tc::kMaxCtas));
-  kern<<<grid, tm::kThreads, smem>>>(mh[0], mh[1], ml[0], ml[1], a);
-  return launch_status();
-}
-
-// Which tensor-core OPW kernel runs: the shared-memory-coefficient kernel unless
-// RCABEAM_DAS_KERNEL=tmem selects the TMEM-coefficient one (a/b timing).
-static bool use_tm_kernel() {
-  const char* v = std::getenv("RCABEAM_DAS_KERNEL");
-  return v && std::string(v) == "tmem";
-}
-
 // MMA steps per float32 accumulation segment (RCABEAM_TC_SEGMENT overrides, for a/b runs).
 static int segment_steps() {
   const char* v = std::getenv("RCABEAM_TC_SEGMENT");
@@ -389,7 +338,6 @@ static int segment_steps() {
 template <bool BF16X3>
 static rcabeam_status run_tc(tc::Args a) {
   a.seg_steps = segment_steps();
-  if (use_tm_kernel()) return run_tm<BF16X3>(a);
   const size_t nt = size_t(a.nt);
   // The deepest ring (one builder warp per stage) that fits shared memory.
   int stages = tc::kDeepStages;
@@ -417,13 +365,7 @@ static rcabeam_status run_tc(tc::Args a) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  // Seven builder warps over the six-stage ring when RCABEAM_TC_BUILDERS=7 (a/b runs;
-  // 12 warps = 3 per SM sub-partition, so the 168-register budget still fits).
-  const char* nb = std::getenv("RCABEAM_TC_BUILDERS");
-  const bool seven = stages == 6 && nb && std::atoi(nb) == 7;
-  const int builders = seven ? 7 : stages;
-  auto kern = seven         ? tc::opw_tc<BF16X3, 6, 7>
-              : stages == 6 ? tc::opw_tc<BF16X3, 6>
+  auto kern = stages == 6   ? tc::opw_tc<BF16X3, 6>
               : stages == 5 ? tc::opw_tc<BF16X3, 5>
               : stages == 4 ? tc::opw_tc<BF16X3, 4>
               : stages == 3 ? tc::opw_tc<BF16X3, 3>
@@ -435,7 +377,7 @@ static rcabeam_status run_tc(tc::Args a) {
   if (!a.partial || !a.slot_clock) return RCABEAM_ERROR_CUDA;
   const int items = a.ntiles * a.chunks;
   const unsigned grid = unsigned(std::min(std::min(items, sms), tc::kMaxCtas));
-  kern<<<grid, tc::threads_for(builders), smem>>>(mh[0], mh[1], ml[0], ml[1], a);
+  kern<<<grid, tc::threads_for(stages), smem>>>(mh[0], mh[1], ml[0], ml[1], a);
   return launch_status();
 }
 
@@ -606,45 +548,9 @@ static void launch_project(const void* iq, void* out, double* power, size_t rows
         reinterpret_cast<const double2*>(vec), int(k), mode, 1.0 / double(nt));
 }
 
-// Streamed projection (complex64 rows, k <= 4, even nt <= 512, 16-byte aligned
-// rows): one CTA per SM, G lanes per row.  False when the form does not apply.
-template <int G, int MAXF>
-static bool launch_project_pipe(const void* iq, void* out, double* power, size_t rows, size_t nt,
-                                const double* vec, size_t k, int mode) {
-  using S = clutter::PipeShape<G>;
-  auto kern = clutter::project_rows_pipe<G, MAXF>;
-  const size_t smem = S::smem_bytes(int(nt));
-  if (smem > 227 * 1024 ||
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
-    return false;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const size_t blocks = (rows + S::kRows - 1) / S::kRows;
-  const size_t per_sm = (MAXF <= 16 && 2 * smem <= 227 * 1024) ? 2 : 1;
-  const unsigned grid = unsigned(std::min<size_t>(blocks, per_sm * size_t(sms)));
-  kern<<<grid, S::kThreads, smem>>>(static_cast<const float2*>(iq), static_cast<float2*>(out), power, rows, int(nt),
-                                    reinterpret_cast<const double2*>(vec), int(k), mode, 1.0 / double(nt),
-                                    device_error_ptr());
-  return true;
-}
-
-static bool project_pipe(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
-                         size_t k, int mode) {
-  if (k > size_t(clutter::kProjSmall) || nt % 2 || nt > 512 || reinterpret_cast<uintptr_t>(iq) % 16 != 0 ||
-      rows > (size_t(1) << 40))
-    return false;
-  // 16 lanes per row, 2 rows per warp, 16-row stages.
-  if (nt <= 256) return launch_project_pipe<16, 16>(iq, out, power, rows, nt, vec, k, mode);
-  return launch_project_pipe<16, 32>(iq, out, power, rows, nt, vec, k, mode);
-}
-
 template <typename IN>
 static void project_dispatch(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
                              size_t k, int mode) {
-  if constexpr (sizeof(IN) == 8) {
-    if (project_pipe(iq, out, power, rows, nt, vec, k, mode)) return;
-  }
   size_t f = (nt + 31) / 32;
   if (f <= 1) launch_project<IN, 1>(iq, out, power, rows, nt, vec, k, mode);
   else if (f <= 2) launch_project<IN, 2>(iq, out, power, rows, nt, vec, k, mode);
