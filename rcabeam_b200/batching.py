@@ -243,7 +243,7 @@ def autotune(ensembles, *, sample_tiles: int = 148 * 2, repeats: int = 2, cache:
         results = {}
         for fpc in FRAME_CHUNKS:
             e.frames_per_chunk = fpc
-            results[fpc] = timed(BatchQueue([e], voxel_limit=_sample(e, sample_tiles)))
+            results[fpc] = timed(BatchQueue([e], ctas_per_sm=3, voxel_limit=_sample(e, sample_tiles)))
         cache[key] = min(results, key=results.get)
     for e in ensembles:
         e.frames_per_chunk = cache[(e.method, e.shape[2], e.shape[3])]

@@ -15,7 +15,12 @@
 // finished per tile by the CTA that completes the tile's last frame chunk, and
 // the CTA that completes an ensemble's last item stamps its completion time.
 // F (16, 32 or 64 frames, the producer's box width) is chosen per ensemble by
-// the caller's autotuner.  All staging loads are plain TMA tile loads.
+// the caller's autotuner; frames past the last whole chunk form one tail chunk
+// of the next power of two >= 4 frames (its own tensor maps), as the
+// single-ensemble launches split them.  A queue whose ensembles share one
+// method runs a kernel compiled for that method alone (no register budget
+// shared with the other methods' paths).  All staging loads are plain TMA tile
+// loads.
 #pragma once
 
 #include "common.cuh"
@@ -32,16 +37,18 @@ struct Ensemble {
   das::Args args;          // pointers, sizes and constants (signal unused)
   int method;              // 0 OPW, 1 XDoppler, 3 DMAS-CCF-ACF
   int lpv;                 // frames per chunk / 2: 8, 16 or 32 (staged methods)
-  int tiles, chunks;       // staged: 64-voxel tiles x frame chunks; DMAS: voxel blocks x 128-frame blocks
+  int lpv_tail;            // tail chunk frames / 2 (2 ... 32), 0 = no tail chunk
+  int tiles, chunks;       // 64-voxel tiles x frame chunks (staged: main chunks + tail; DMAS: 32-frame chunks)
+  int main_chunks;         // whole F-frame chunks
   int tma;                 // tensor maps valid (else plain staging loads)
-  int pad;
+  int chunk_major;         // item order within the ensemble: chunk-major (1) or tile-major (0)
   long long first_item;    // items before this ensemble
   long long tile_base;     // first per-tile counter of this ensemble
 };
 
 struct Queue {
   const Ensemble* ens;
-  const CUtensorMap* maps;       // [2 n]: RC, CR (64-byte aligned)
+  const CUtensorMap* maps;       // [4 n]: RC, CR main chunks, RC, CR tail chunk (64-byte aligned)
   int n;
   long long total_items;
   unsigned long long* next;      // work counter
@@ -66,17 +73,38 @@ struct Smem {
   static constexpr size_t kBytes = kAngles + size_t(kMaxAngles) * 3 * sizeof(double);
 };
 
-template <int LPV>
+// KIND: the queue's one method (0 OPW, 1 XDoppler, 3 DMAS), or -1 for a mixed queue.
+template <int LPV, int KIND>
 __device__ __forceinline__ bool staged(const Queue& q, const Ensemble& e, int ei, const das::Ring& ring,
-                                       const unsigned* vox, const double* angle_tab, int frame0, uint32_t& k) {
+                                       const unsigned* vox, const double* angle_tab, int frame0, bool tail,
+                                       uint32_t& k) {
   const int warp = threadIdx.x >> 5;
   if (warp == das::kConsumerWarps) {
-    const CUtensorMap* mr = q.maps + 2 * ei;
+    const CUtensorMap* mr = q.maps + 4 * ei + (tail ? 2 : 0);
     if (e.tma) return das::produce_item<LPV, false, true>(mr, mr + 1, e.args, vox, angle_tab, ring, frame0, k);
     return das::produce_item<LPV, false, false>(mr, mr + 1, e.args, vox, angle_tab, ring, frame0, k);
   }
-  if (e.method == 1) return das::consume_item<LPV, false, das::kXdoppler>(e.args, vox, ring, frame0, warp, k);
-  return das::consume_item<LPV, false, das::kOpw>(e.args, vox, ring, frame0, warp, k);
+  if constexpr (KIND == 1) {
+    return das::consume_item<LPV, false, das::kXdoppler>(e.args, vox, ring, frame0, warp, k);
+  } else if constexpr (KIND == 0) {
+    return das::consume_item<LPV, false, das::kOpw>(e.args, vox, ring, frame0, warp, k);
+  } else {
+    if (e.method == 1) return das::consume_item<LPV, false, das::kXdoppler>(e.args, vox, ring, frame0, warp, k);
+    return das::consume_item<LPV, false, das::kOpw>(e.args, vox, ring, frame0, warp, k);
+  }
+}
+
+template <int KIND>
+__device__ __forceinline__ bool staged_any(int lpv, const Queue& q, const Ensemble& e, int ei, const das::Ring& ring,
+                                           const unsigned* vox, const double* angle_tab, int frame0, bool tail,
+                                           uint32_t& k) {
+  switch (lpv) {
+    case 32: return staged<32, KIND>(q, e, ei, ring, vox, angle_tab, frame0, tail, k);
+    case 16: return staged<16, KIND>(q, e, ei, ring, vox, angle_tab, frame0, tail, k);
+    case 8: return staged<8, KIND>(q, e, ei, ring, vox, angle_tab, frame0, tail, k);
+    case 4: return staged<4, KIND>(q, e, ei, ring, vox, angle_tab, frame0, tail, k);
+    default: return staged<2, KIND>(q, e, ei, ring, vox, angle_tab, frame0, tail, k);
+  }
 }
 
 // DMAS-CCF-ACF item: 64-voxel tile x 32-frame chunk, both passes through the ring.
@@ -85,7 +113,7 @@ __device__ __forceinline__ bool staged_dmas(const Queue& q, const Ensemble& e, i
                                             uint32_t& k) {
   const int warp = threadIdx.x >> 5;
   if (warp == das::kConsumerWarps) {
-    const CUtensorMap* mr = q.maps + 2 * ei;
+    const CUtensorMap* mr = q.maps + 4 * ei;
     if (e.tma)
       return das::produce_dmas_item<kDmasLpv, true>(mr, mr + 1, e.args, vox, angle_tab, ring, frame0, k, active);
     return das::produce_dmas_item<kDmasLpv, false>(mr, mr + 1, e.args, vox, angle_tab, ring, frame0, k, active);
@@ -94,8 +122,8 @@ __device__ __forceinline__ bool staged_dmas(const Queue& q, const Ensemble& e, i
 }
 
 // MINB resident CTAs per SM (register budget 65536 / (288 MINB)); the
-// autotuner picks the variant.
-template <int MINB>
+// autotuner picks the variant.  KIND as for staged().
+template <int MINB, int KIND>
 __global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const das::Ring ring{smem + Smem::kData, 0, reinterpret_cast<das::StageTap*>(smem + Smem::kTaps),
@@ -140,21 +168,25 @@ __global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q) {
     const int ei = *ens_slot;
     const Ensemble& e = q.ens[ei];
     const long long local = item - e.first_item;
-    const int tile = int(local / e.chunks), chunk = int(local % e.chunks);
+    const int tile = e.chunk_major ? int(local % e.tiles) : int(local / e.chunks);
+    const int chunk = e.chunk_major ? int(local / e.tiles) : int(local % e.chunks);
     bool ok = true;
     {
       das::load_item_tables(e.args, size_t(tile) * das::kTileVoxels, vox, angle_tab);
       __syncthreads();
       das::Ring r = ring;
-      r.slot_bytes = size_t(das::kRows) * (2 * e.lpv) * 8;
       const int frame0 = chunk * 2 * e.lpv;
-      if (e.method == 3) {
-        ok = staged_dmas(q, e, ei, r, vox, active, angle_tab, frame0, k);
+      if (KIND == 3 || (KIND < 0 && e.method == 3)) {
+        if constexpr (KIND == 3 || KIND < 0) {
+          r.slot_bytes = size_t(das::kRows) * (2 * kDmasLpv) * 8;
+          ok = staged_dmas(q, e, ei, r, vox, active, angle_tab, chunk * 2 * kDmasLpv, k);
+        }
       } else {
-        switch (e.lpv) {
-          case 8: ok = staged<8>(q, e, ei, r, vox, angle_tab, frame0, k); break;
-          case 16: ok = staged<16>(q, e, ei, r, vox, angle_tab, frame0, k); break;
-          default: ok = staged<32>(q, e, ei, r, vox, angle_tab, frame0, k); break;
+        if constexpr (KIND != 3) {
+          const bool tail = chunk == e.main_chunks;
+          const int lpv = tail ? e.lpv_tail : e.lpv;
+          r.slot_bytes = size_t(das::kRows) * (2 * lpv) * 8;
+          ok = staged_any<KIND>(lpv, q, e, ei, r, vox, angle_tab, frame0, tail, k);
         }
       }
     }
@@ -162,7 +194,7 @@ __global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q) {
     __syncthreads();  // every warp's results of this item are issued
     if (threadIdx.x == 0) {
       __threadfence();
-      if (e.method == 1) {
+      if (KIND == 1 || (KIND < 0 && e.method == 1)) {
         // Last chunk of this tile: XDoppler magnitude |mean r conj(q)| of its voxels.
         const unsigned c = atomicAdd(q.tile_done + e.tile_base + tile, 1u) + 1;
         if (c == unsigned(e.chunks)) *item_slot = -1;  // flag for the block below
@@ -171,7 +203,7 @@ __global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q) {
       if (d == unsigned(e.tiles) * unsigned(e.chunks)) q.times[1 + ei] = global_ns();
     }
     __syncthreads();
-    if (e.method == 1 && *item_slot == -1) {
+    if ((KIND == 1 || (KIND < 0 && e.method == 1)) && *item_slot == -1) {
       __threadfence();
       for (int i = threadIdx.x; i < das::kTileVoxels; i += blockDim.x) {
         const unsigned v = vox[i];

@@ -73,7 +73,6 @@ struct Unit {
 
 struct Params {
   int nunits, slices, nload_max, nt;
-  int tf32_swizzle;  // direct TF32 operand layout: granule ^= (row & 3) (0) or ((row >> 1) & 3) (1)
   long long rows, slice_rows;
   const double* scale;
   double* upper;
@@ -316,239 +315,6 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc(const __grid_constant__ C
               const float o_re = __shfl_xor_sync(0xffffffffu, val[2 * i], 1);
               const float o_im = __shfl_xor_sync(0xffffffffu, val[2 * i + 1], 1);
               // Even row 2m holds (D[2m][2n], D[2m][2n+1]); its partner row 2m+1 the same columns.
-              const int n = (u.b_blk[t] * kBlock + c0) / 2 + i;
-              if (even && m < p.nt && n < p.nt) {
-                const double re = double(val[2 * i]) + double(o_im);
-                const double im = double(val[2 * i + 1]) - double(o_re);
-                atomicAdd(p.upper + 2 * (size_t(m) * p.nt + n), re * factor);
-                atomicAdd(p.upper + 2 * (size_t(m) * p.nt + n) + 1, im * factor);
-              }
-            }
-          }
-        }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(acc_empty);
-        ++flushes;
-      }
-    }
-  }
-  __syncthreads();
-  if (warp == 1) {
-    tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
-  }
-}
-
-// Tensor-core Gram with the converters loading rows straight from global memory.
-// gram_tc<false> stages every float32 row block in shared memory by TMA and
-// the converters read it back before writing the BF16 hi / lo operands: per
-// 16-row stage that is 48 KB written + 48 KB read on top of the 48 KB of
-// operands written and the 96 KB the MMAs read, which bounds the kernel by
-// shared-memory bandwidth, not the tensor pipe.  Here seven converter warps
-// (every warp but the MMA warp) load their 8-column pieces with 16-byte global
-// loads one stage ahead in registers, split them and store only the operands
-// (a 3-stage operand ring).  Same units, operand layouts, MMAs and epilogue as
-// gram_tc, so the same sums in the same order.  TF32 operands (rounded to
-// nearest) are written in the layout the TMA's 32-byte-granule 128-byte swizzle
-// gives gram_tc<true>.
-constexpr int kDirectRing = 3;
-constexpr int kDirectWarps = 7;
-constexpr int kDirectConverters = kDirectWarps * 32;
-constexpr int kDirectItems = (kMaxLoads * kRows * 16 + kDirectConverters - 1) / kDirectConverters;  // 7
-
-__host__ __device__ inline size_t direct_smem_bytes(int nload_max) {
-  return size_t(kDirectRing) * nload_max * kSlotBytes + 1024 + 1024;
-}
-
-template <bool TF32>
-__global__ void __launch_bounds__(kThreads, 1) gram_direct(const float* __restrict__ y, const Params p) {
-  using namespace rcb::tc;
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const Unit& u = p.units[blockIdx.x % p.nunits];
-  const int slice = blockIdx.x / p.nunits;
-  const size_t stage_bytes = size_t(p.nload_max) * kSlotBytes;
-  unsigned char* operands = smem;
-  uint64_t* op_full = reinterpret_cast<uint64_t*>(operands + kDirectRing * stage_bytes);
-  uint64_t* op_empty = op_full + kDirectRing;
-  uint64_t* acc_full = op_empty + kDirectRing;
-  uint64_t* acc_empty = acc_full + 1;
-  uint64_t* drain = acc_empty + 1;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long r0 = (long long)slice * p.slice_rows;
-  const long long r1 = r0 + p.slice_rows < p.rows ? r0 + p.slice_rows : p.rows;
-  const int nstages = r1 > r0 ? int((r1 - r0 + kRows - 1) / kRows) : 0;
-  constexpr int kStagesPerFlush = kFlushRows / kRows;
-  const long long cols = 2ll * p.nt;  // real columns of a row
-
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < kDirectRing; ++s) {
-      mbar_init(&op_full[s], kDirectWarps);
-      mbar_init(&op_empty[s], 1);
-    }
-    mbar_init(acc_full, 1);
-    mbar_init(acc_empty, 4);
-    mbar_init(drain, 1);
-    fence_mbar_init();
-  }
-  if (warp == 1) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(kTmemCols)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = *tmem_slot;
-
-  const double s = *p.scale;
-  int e = 0;
-  if (s > 0.0 && s <= 1.79e308) frexp(s, &e);
-  const float prescale = s > 0.0 ? float(ldexp(1.0, -e)) : 1.0f;
-  const double factor = s > 0.0 ? (ldexp(1.0, e) / s) * (ldexp(1.0, e) / s) : 1.0;
-
-  if (warp == 1) {
-    // ------------------------------------------------------------------ MMA --
-    if (lane == 0) {
-      const uint32_t idesc = idesc_mn(TF32, 128, 128);
-      int flushes = 0;
-      for (int k = 0; k < nstages; ++k) {
-        const int s_ = k % kDirectRing;
-        const int in_seg = k % kStagesPerFlush;
-        if (in_seg == 0 && flushes > 0 && !mbar_wait(acc_empty, (flushes - 1) & 1, p.err, kErrWaitEmpty)) break;
-        if (!mbar_wait(&op_full[s_], (k / kDirectRing) & 1, p.err, kErrWaitFull)) break;
-        tc_fence_after();
-        const uint32_t op = smem_u32(operands + s_ * stage_bytes);
-        for (int t = 0; t < u.ntask; ++t) {
-          const uint32_t d = tmem + uint32_t(kBlock * t);
-          if constexpr (TF32) {
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-              const uint32_t a = op + u.a_slot[t] * kSlotBytes + q * 1024;
-              const uint32_t b = op + u.b_slot[t] * kSlotBytes + q * 1024;
-              mma_tf32(d, smem_desc(a, 2048, 512, kLayoutSw128Base32), smem_desc(b, 2048, 512, kLayoutSw128Base32),
-                       idesc, (in_seg > 0 || q > 0) ? 1u : 0u);
-            }
-          } else {
-            const uint32_t hi = op, lo = op + uint32_t(p.nload_max) * (kSlotBytes / 2);
-            const uint32_t ah = hi + u.a_slot[t] * (kSlotBytes / 2), al = lo + u.a_slot[t] * (kSlotBytes / 2);
-            const uint32_t bh = hi + u.b_slot[t] * (kSlotBytes / 2), bl = lo + u.b_slot[t] * (kSlotBytes / 2);
-            mma_f16(d, smem_desc(ah, 2048, 1024, kLayoutSw128), smem_desc(bh, 2048, 1024, kLayoutSw128), idesc,
-                    in_seg > 0 ? 1u : 0u);
-            mma_f16(d, smem_desc(al, 2048, 1024, kLayoutSw128), smem_desc(bh, 2048, 1024, kLayoutSw128), idesc, 1u);
-            mma_f16(d, smem_desc(ah, 2048, 1024, kLayoutSw128), smem_desc(bl, 2048, 1024, kLayoutSw128), idesc, 1u);
-          }
-        }
-        mma_commit(&op_empty[s_]);
-        if (in_seg == kStagesPerFlush - 1 || k == nstages - 1) {
-          mma_commit(acc_full);
-          ++flushes;
-        }
-      }
-      mma_commit(drain);
-      mbar_wait(drain, 0, p.err, kErrWaitDrain);
-    }
-    __syncwarp();
-  } else {
-    // ------------------------------------------------ converters / epilogue --
-    const int ct = warp == 0 ? lane : (warp - 1) * 32 + lane;  // 0 .. 223
-    const bool epilogue = warp >= 4;
-    const int quarter = warp & 3;
-    const int items = u.nload * kRows * 16;  // (slot, row, 64-column atom, 8-column chunk)
-    int flushes = 0;
-    float4 cur[kDirectItems][2], nxt[kDirectItems][2];
-    // The 8 float32 columns of every item of stage k (zeros past the rows or columns).
-    auto fetch = [&](float4 (&buf)[kDirectItems][2], int k) {
-      const long long rbase = r0 + (long long)k * kRows;
-#pragma unroll
-      for (int j = 0; j < kDirectItems; ++j) {
-        const int i = ct + j * kDirectConverters;
-        buf[j][0] = make_float4(0.f, 0.f, 0.f, 0.f);
-        buf[j][1] = buf[j][0];
-        if (i < items) {
-          const int slot = i >> 8, rem = i & 255;
-          const int row = rem >> 4;
-          // 8 columns: BF16 (64-column atom, 8-column chunk) or TF32 (32-column box, 32-byte granule).
-          const int piece = TF32 ? (((rem >> 2) & 3) * 32 + (rem & 3) * 8) : (((rem >> 3) & 1) * 64 + (rem & 7) * 8);
-          const long long r = rbase + row;
-          const long long col = (long long)u.load[slot] * kBlock + piece;
-          if (r < r1 && col < cols) {
-            const float4* src = reinterpret_cast<const float4*>(y + r * cols + col);
-            buf[j][0] = __ldg(src);
-            if (col + 4 < cols) buf[j][1] = __ldg(src + 1);
-          }
-        }
-      }
-    };
-    if (nstages > 0) fetch(cur, 0);
-    for (int k = 0; k < nstages; ++k) {
-      const int s_ = k % kDirectRing;
-      if (k + 1 < nstages) fetch(nxt, k + 1);
-      if (k >= kDirectRing &&
-          !__all_sync(0xffffffffu, mbar_wait(&op_empty[s_], ((k / kDirectRing) - 1) & 1, p.err, kErrWaitEmpty)))
-        break;
-      unsigned char* hi = operands + s_ * stage_bytes;
-      unsigned char* lo = hi + size_t(p.nload_max) * (kSlotBytes / 2);
-#pragma unroll
-      for (int j = 0; j < kDirectItems; ++j) {
-        const int i = ct + j * kDirectConverters;
-        if (i < items) {
-          const int slot = i >> 8, rem = i & 255;
-          const int row = rem >> 4;
-          const float4 x0 = cur[j][0], x1 = cur[j][1];
-          if constexpr (TF32) {
-            // MN-major 128-byte swizzle with 32-byte granules: 32-column boxes of 16 rows x 128 B,
-            // granule g of row r at (g ^ (r & 3)) x 32 B (4-row atoms, SBO = 512 B).
-            const int box = (rem >> 2) & 3, g = rem & 3;
-            const int sw = p.tf32_swizzle ? ((row >> 1) & 3) : (row & 3);
-            const int off = slot * kSlotBytes + box * 2048 + row * 128 + ((g ^ sw) << 5);
-            const float4 a = make_float4(round_tf32(x0.x * prescale), round_tf32(x0.y * prescale),
-                                         round_tf32(x0.z * prescale), round_tf32(x0.w * prescale));
-            const float4 b = make_float4(round_tf32(x1.x * prescale), round_tf32(x1.y * prescale),
-                                         round_tf32(x1.z * prescale), round_tf32(x1.w * prescale));
-            *reinterpret_cast<float4*>(hi + off) = a;
-            *reinterpret_cast<float4*>(hi + off + 16) = b;
-          } else {
-            const int atom = (rem >> 3) & 1, c = rem & 7;
-            const int sw = row & 7;
-            const float v[8] = {x0.x * prescale, x0.y * prescale, x0.z * prescale, x0.w * prescale,
-                                x1.x * prescale, x1.y * prescale, x1.z * prescale, x1.w * prescale};
-            uint4 h, l;
-            split8(v, h, l);
-            const int off = slot * (kSlotBytes / 2) + atom * 2048 + (row >> 3) * 1024 + sw * 128 + ((c ^ sw) << 4);
-            *reinterpret_cast<uint4*>(hi + off) = h;
-            *reinterpret_cast<uint4*>(lo + off) = l;
-          }
-        }
-      }
-      fence_async_smem();  // generic-proxy writes -> visible to the tensor core
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&op_full[s_]);
-#pragma unroll
-      for (int j = 0; j < kDirectItems; ++j) {
-        cur[j][0] = nxt[j][0];
-        cur[j][1] = nxt[j][1];
-      }
-      const bool flush_here = (k % kStagesPerFlush) == kStagesPerFlush - 1 || k == nstages - 1;
-      if (epilogue && flush_here) {
-        if (!__all_sync(0xffffffffu, mbar_wait(acc_full, flushes & 1, p.err, kErrWaitFull))) break;
-        tc_fence_after();
-        const int m_lane = 32 * quarter + lane;
-        const bool even = (lane & 1) == 0;
-        for (int t = 0; t < u.ntask; ++t) {
-          const int row_real = u.a_blk[t] * kBlock + m_lane;
-          const int m = row_real >> 1;
-          for (int c0 = 0; c0 < kBlock; c0 += 32) {
-            float val[32];
-            tmem_ld32(tmem + (uint32_t(32 * quarter) << 16) + uint32_t(kBlock * t + c0), val);
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-              const float o_re = __shfl_xor_sync(0xffffffffu, val[2 * i], 1);
-              const float o_im = __shfl_xor_sync(0xffffffffu, val[2 * i + 1], 1);
               const int n = (u.b_blk[t] * kBlock + c0) / 2 + i;
               if (even && m < p.nt && n < p.nt) {
                 const double re = double(val[2 * i]) + double(o_im);

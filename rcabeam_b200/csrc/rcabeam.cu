@@ -689,14 +689,6 @@ rcabeam_status rcabeam_clutter_scale_device(const void* iq, size_t n, int comple
 // Tensor-core Gram (precision 2 = TF32, 3 = 3xBF16) of a complex64 Casorati
 // matrix: the rows x 2T float32 view as a 2-D tensor with 32 x 16 SWIZZLE_128B
 // boxes, one CTA per (unit, row slice).
-// Direct-load Gram for 3xBF16 unless RCABEAM_GRAM_KERNEL=staged; for TF32 only with
-// RCABEAM_GRAM_KERNEL=direct (a/b timing while its operand layout is being checked).
-static bool gram_direct(bool tf32) {
-  const char* v = std::getenv("RCABEAM_GRAM_KERNEL");
-  const std::string kind = v ? v : "";
-  return tf32 ? (kind == "direct" || kind == "direct2") : kind != "staged";
-}
-
 static rcabeam_status gram_tc_launch(const void* iq, size_t rows, size_t nt, const double* scale, bool tf32,
                                      double* upper) {
   auto fn = encode_fn();
@@ -726,19 +718,6 @@ static rcabeam_status gram_tc_launch(const void* iq, size_t rows, size_t nt, con
          CU_TENSOR_MAP_INTERLEAVE_NONE, tf32 ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B : CU_TENSOR_MAP_SWIZZLE_128B,
          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return RCABEAM_ERROR_ARGUMENT;
-  {
-    const char* v = std::getenv("RCABEAM_GRAM_KERNEL");
-    prm.tf32_swizzle = v && std::string(v) == "direct2" ? 1 : 0;
-  }
-  if (gram_direct(tf32)) {
-    // Converters load the rows from global memory (no TMA staging).
-    const size_t smem = std::max(gramtc::direct_smem_bytes(prm.nload_max), size_t(120) << 10);
-    auto kern = tf32 ? gramtc::gram_direct<true> : gramtc::gram_direct<false>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
-      return RCABEAM_ERROR_CUDA;
-    kern<<<unsigned(prm.nunits * prm.slices), gramtc::kThreads, smem>>>(static_cast<const float*>(iq), prm);
-    return launch_status();
-  }
   // At least 120 KB keeps one CTA (and one 512-column TMEM allocation) per SM.
   const size_t smem = std::max(gramtc::smem_bytes(prm.nload_max), size_t(120) << 10);
   auto kern = tf32 ? gramtc::gram_tc<true> : gramtc::gram_tc<false>;
@@ -1260,8 +1239,16 @@ bool batch_plan(size_t n, const rcabeam_batch_ensemble* list, std::vector<batch:
       e.tiles = int((d.nv + das::kTileVoxels - 1) / das::kTileVoxels);
       e.chunks = int((d.nt + 2 * batch::kDmasLpv - 1) / (2 * batch::kDmasLpv));
     } else {
+      // Whole F-frame chunks, then one tail chunk of the next power of two >= 4 frames.
       e.tiles = int((d.nv + das::kTileVoxels - 1) / das::kTileVoxels);
-      e.chunks = int((d.nt + fpc - 1) / fpc);
+      e.main_chunks = int(d.nt / fpc);
+      const unsigned tail = unsigned(d.nt % fpc);
+      e.lpv_tail = tail ? int(std::max(pow2_at_least(tail), 4u) / 2) : 0;
+      e.chunks = e.main_chunks + (tail ? 1 : 0);
+    }
+    {
+      const char* order = std::getenv("RCABEAM_BATCH_ORDER");
+      e.chunk_major = order && std::string(order) == "chunk" ? 1 : 0;
     }
     e.tma = (d.nt * 8) % 16 == 0 && reinterpret_cast<uintptr_t>(d.rc) % 16 == 0 &&
             reinterpret_cast<uintptr_t>(d.cr) % 16 == 0 && encode_fn() != nullptr;
@@ -1295,7 +1282,7 @@ bool batch_plan(size_t n, const rcabeam_batch_ensemble* list, std::vector<batch:
   }
   L->ens = 0;
   L->maps = align256(n * sizeof(batch::Ensemble));
-  L->next = L->maps + align256(2 * n * sizeof(CUtensorMap));
+  L->next = L->maps + align256(4 * n * sizeof(CUtensorMap));
   L->done = L->next + 256;
   L->tile_done = L->done + align256(n * 4);
   L->total = L->tile_done + align256(size_t(tiles_xd > 0 ? tiles_xd : 1) * 4);
@@ -1337,20 +1324,22 @@ rcabeam_status rcabeam_batch_prepare(size_t n, const rcabeam_batch_ensemble* lis
   if (!table || reinterpret_cast<uintptr_t>(table) % 256 != 0 || !batch_plan(n, list, &ens, &L, &total) ||
       table_bytes < L.total)
     return RCABEAM_ERROR_ARGUMENT;
-  std::vector<CUtensorMap> maps(2 * n);
+  std::vector<CUtensorMap> maps(4 * n);
   for (size_t i = 0; i < n; ++i) {
     batch::Ensemble& e = ens[i];
     if (!e.tma) continue;
-    const int frames = 2 * e.lpv;
-    const size_t slabs = size_t(e.args.nc) * e.args.na;
-    if (!make_slab_map(&maps[2 * i], e.args.rc, 8, size_t(e.args.nt), size_t(e.args.ns), slabs, frames, das::kRows) ||
-        !make_slab_map(&maps[2 * i + 1], e.args.cr, 8, size_t(e.args.nt), size_t(e.args.ns), slabs, frames,
-                       das::kRows))
-      e.tma = 0;
+    const size_t slabs = size_t(e.args.nc) * e.args.na, nt = size_t(e.args.nt), ns = size_t(e.args.ns);
+    for (int part = 0; part < 2; ++part) {
+      const int frames = 2 * (part ? e.lpv_tail : e.lpv);
+      if (!frames) continue;
+      if (!make_slab_map(&maps[4 * i + 2 * part], e.args.rc, 8, nt, ns, slabs, frames, das::kRows) ||
+          !make_slab_map(&maps[4 * i + 2 * part + 1], e.args.cr, 8, nt, ns, slabs, frames, das::kRows))
+        e.tma = 0;
+    }
   }
   unsigned char* t = static_cast<unsigned char*>(table);
   if (cudaMemcpy(t + L.ens, ens.data(), n * sizeof(batch::Ensemble), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(t + L.maps, maps.data(), 2 * n * sizeof(CUtensorMap), cudaMemcpyHostToDevice) != cudaSuccess)
+      cudaMemcpy(t + L.maps, maps.data(), 4 * n * sizeof(CUtensorMap), cudaMemcpyHostToDevice) != cudaSuccess)
     return RCABEAM_ERROR_CUDA;
   return RCABEAM_SUCCESS;
 }
@@ -1374,7 +1363,18 @@ rcabeam_status rcabeam_batch_run_device(size_t n, const rcabeam_batch_ensemble* 
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  auto kern = ctas_per_sm == 1 ? batch::run<1> : ctas_per_sm == 2 ? batch::run<2> : batch::run<3>;
+  // A queue of one method runs the kernel compiled for that method alone.
+  int kind = list[0].method;
+  for (size_t i = 1; i < n; ++i)
+    if (list[i].method != kind) kind = -1;
+  using Kernel = void (*)(const batch::Queue);
+  static const Kernel kernels[4][3] = {
+      {batch::run<1, -1>, batch::run<2, -1>, batch::run<3, -1>},
+      {batch::run<1, 0>, batch::run<2, 0>, batch::run<3, 0>},
+      {batch::run<1, 1>, batch::run<2, 1>, batch::run<3, 1>},
+      {batch::run<1, 3>, batch::run<2, 3>, batch::run<3, 3>},
+  };
+  const Kernel kern = kernels[kind < 0 ? 0 : kind == 3 ? 3 : kind + 1][ctas_per_sm - 1];
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(batch::Smem::kBytes)) !=
       cudaSuccess)
     return RCABEAM_ERROR_CUDA;

@@ -36,6 +36,7 @@ SPECS = [  # method, depth points, frames, angles
     ("xdoppler", 20, 10, 5),
     ("dmas", 9, 130, 2),
     ("opw", 7, 2, 1),
+    ("xdoppler", 6, 71, 2),  # a 7-frame tail chunk for every chunk width
 ]
 
 
