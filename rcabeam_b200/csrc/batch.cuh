@@ -58,9 +58,10 @@ struct Queue {
   int* err;
 };
 
+// Shared-memory layout for slots of up to 2 LPV frames.
+template <int LPV>
 struct Smem {
-  static constexpr int kLpv = 32;
-  using S = das::Shape<kLpv, false>;
+  using S = das::Shape<LPV, false>;
   static constexpr size_t kData = 0;
   static constexpr size_t kTaps = size_t(das::kStages) * S::kStageBytes;
   static constexpr size_t kMeta = kTaps + size_t(das::kStages) * das::kTileVoxels * sizeof(das::StageTap);
@@ -75,56 +76,60 @@ struct Smem {
 
 // KIND: the queue's one method (0 OPW, 1 XDoppler, 3 DMAS), or -1 for a mixed queue.
 template <int LPV, int KIND>
-__device__ __forceinline__ bool staged(const Queue& q, const Ensemble& e, int ei, const das::Ring& ring,
-                                       const unsigned* vox, const double* angle_tab, int frame0, bool tail,
-                                       uint32_t& k) {
+__device__ __forceinline__ bool staged(const Queue& q, const das::Args& args, int method, int tma, int ei,
+                                       const das::Ring& ring, const unsigned* vox, const double* angle_tab,
+                                       int frame0, bool tail, uint32_t& k) {
   const int warp = threadIdx.x >> 5;
   if (warp == das::kConsumerWarps) {
     const CUtensorMap* mr = q.maps + 4 * ei + (tail ? 2 : 0);
-    if (e.tma) return das::produce_item<LPV, false, true>(mr, mr + 1, e.args, vox, angle_tab, ring, frame0, k);
-    return das::produce_item<LPV, false, false>(mr, mr + 1, e.args, vox, angle_tab, ring, frame0, k);
+    if (tma) return das::produce_item<LPV, false, true>(mr, mr + 1, args, vox, angle_tab, ring, frame0, k);
+    return das::produce_item<LPV, false, false>(mr, mr + 1, args, vox, angle_tab, ring, frame0, k);
   }
   if constexpr (KIND == 1) {
-    return das::consume_item<LPV, false, das::kXdoppler>(e.args, vox, ring, frame0, warp, k);
+    return das::consume_item<LPV, false, das::kXdoppler>(args, vox, ring, frame0, warp, k);
   } else if constexpr (KIND == 0) {
-    return das::consume_item<LPV, false, das::kOpw>(e.args, vox, ring, frame0, warp, k);
+    return das::consume_item<LPV, false, das::kOpw>(args, vox, ring, frame0, warp, k);
   } else {
-    if (e.method == 1) return das::consume_item<LPV, false, das::kXdoppler>(e.args, vox, ring, frame0, warp, k);
-    return das::consume_item<LPV, false, das::kOpw>(e.args, vox, ring, frame0, warp, k);
+    if (method == 1) return das::consume_item<LPV, false, das::kXdoppler>(args, vox, ring, frame0, warp, k);
+    return das::consume_item<LPV, false, das::kOpw>(args, vox, ring, frame0, warp, k);
   }
 }
 
 template <int KIND>
-__device__ __forceinline__ bool staged_any(int lpv, const Queue& q, const Ensemble& e, int ei, const das::Ring& ring,
-                                           const unsigned* vox, const double* angle_tab, int frame0, bool tail,
-                                           uint32_t& k) {
+__device__ __forceinline__ bool staged_any(int lpv, const Queue& q, const das::Args& args, int method, int tma,
+                                           int ei, const das::Ring& ring, const unsigned* vox,
+                                           const double* angle_tab, int frame0, bool tail, uint32_t& k) {
   switch (lpv) {
-    case 32: return staged<32, KIND>(q, e, ei, ring, vox, angle_tab, frame0, tail, k);
-    case 16: return staged<16, KIND>(q, e, ei, ring, vox, angle_tab, frame0, tail, k);
-    case 8: return staged<8, KIND>(q, e, ei, ring, vox, angle_tab, frame0, tail, k);
-    case 4: return staged<4, KIND>(q, e, ei, ring, vox, angle_tab, frame0, tail, k);
-    default: return staged<2, KIND>(q, e, ei, ring, vox, angle_tab, frame0, tail, k);
+    case 32: return staged<32, KIND>(q, args, method, tma, ei, ring, vox, angle_tab, frame0, tail, k);
+    case 16: return staged<16, KIND>(q, args, method, tma, ei, ring, vox, angle_tab, frame0, tail, k);
+    case 8: return staged<8, KIND>(q, args, method, tma, ei, ring, vox, angle_tab, frame0, tail, k);
+    case 4: return staged<4, KIND>(q, args, method, tma, ei, ring, vox, angle_tab, frame0, tail, k);
+    default: return staged<2, KIND>(q, args, method, tma, ei, ring, vox, angle_tab, frame0, tail, k);
   }
 }
 
 // DMAS-CCF-ACF item: 64-voxel tile x 32-frame chunk, both passes through the ring.
-__device__ __forceinline__ bool staged_dmas(const Queue& q, const Ensemble& e, int ei, const das::Ring& ring,
-                                            const unsigned* vox, float* active, const double* angle_tab, int frame0,
-                                            uint32_t& k) {
+__device__ __forceinline__ bool staged_dmas(const Queue& q, const das::Args& args, int tma, int ei,
+                                            const das::Ring& ring, const unsigned* vox, float* active,
+                                            const double* angle_tab, int frame0, uint32_t& k) {
   const int warp = threadIdx.x >> 5;
   if (warp == das::kConsumerWarps) {
     const CUtensorMap* mr = q.maps + 4 * ei;
-    if (e.tma)
-      return das::produce_dmas_item<kDmasLpv, true>(mr, mr + 1, e.args, vox, angle_tab, ring, frame0, k, active);
-    return das::produce_dmas_item<kDmasLpv, false>(mr, mr + 1, e.args, vox, angle_tab, ring, frame0, k, active);
+    if (tma) return das::produce_dmas_item<kDmasLpv, true>(mr, mr + 1, args, vox, angle_tab, ring, frame0, k, active);
+    return das::produce_dmas_item<kDmasLpv, false>(mr, mr + 1, args, vox, angle_tab, ring, frame0, k, active);
   }
-  return das::consume_dmas_item<kDmasLpv>(e.args, vox, active, ring, frame0, warp, k);
+  return das::consume_dmas_item<kDmasLpv>(args, vox, active, ring, frame0, warp, k);
 }
 
 // MINB resident CTAs per SM (register budget 65536 / (288 MINB)); the
 // autotuner picks the variant.  KIND as for staged().
+// Slot width of a queue of kind KIND: 32-frame slots for DMAS alone, else 64.
+template <int KIND>
+__host__ __device__ constexpr int smem_lpv() { return KIND == 3 ? kDmasLpv : 32; }
+
 template <int MINB, int KIND>
 __global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q) {
+  using Smem = batch::Smem<smem_lpv<KIND>()>;
   extern __shared__ __align__(1024) unsigned char smem[];
   const das::Ring ring{smem + Smem::kData, 0, reinterpret_cast<das::StageTap*>(smem + Smem::kTaps),
                        reinterpret_cast<int*>(smem + Smem::kMeta), reinterpret_cast<uint64_t*>(smem + Smem::kFull),
@@ -172,21 +177,25 @@ __global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q) {
     const int chunk = e.chunk_major ? int(local / e.tiles) : int(local % e.chunks);
     bool ok = true;
     {
-      das::load_item_tables(e.args, size_t(tile) * das::kTileVoxels, vox, angle_tab);
+      // A private copy: the table in global memory could alias the stores of
+      // the item, so its fields would be reloaded inside the hot loops.
+      const das::Args args = e.args;
+      const int method = e.method, tma = e.tma;
+      das::load_item_tables(args, size_t(tile) * das::kTileVoxels, vox, angle_tab);
       __syncthreads();
       das::Ring r = ring;
       const int frame0 = chunk * 2 * e.lpv;
-      if (KIND == 3 || (KIND < 0 && e.method == 3)) {
+      if (KIND == 3 || (KIND < 0 && method == 3)) {
         if constexpr (KIND == 3 || KIND < 0) {
           r.slot_bytes = size_t(das::kRows) * (2 * kDmasLpv) * 8;
-          ok = staged_dmas(q, e, ei, r, vox, active, angle_tab, chunk * 2 * kDmasLpv, k);
+          ok = staged_dmas(q, args, tma, ei, r, vox, active, angle_tab, chunk * 2 * kDmasLpv, k);
         }
       } else {
         if constexpr (KIND != 3) {
           const bool tail = chunk == e.main_chunks;
           const int lpv = tail ? e.lpv_tail : e.lpv;
           r.slot_bytes = size_t(das::kRows) * (2 * lpv) * 8;
-          ok = staged_any<KIND>(lpv, q, e, ei, r, vox, angle_tab, frame0, tail, k);
+          ok = staged_any<KIND>(lpv, q, args, method, tma, ei, r, vox, angle_tab, frame0, tail, k);
         }
       }
     }

@@ -343,6 +343,106 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// Lane-group form of the small projection (k <= kProjSmall, nt <= L * MAXF):
+// L lanes per row (32 / L rows per warp), lane q holding frames q, q + L, ...
+// widened to float64 once, in registers, for both passes.  The k vectors are
+// staged in shared memory once per persistent CTA, so a row costs one read of
+// its samples and shared-memory broadcasts of the vectors (project_rows_one
+// reloads them through L1 for every row, twice).  The sums run over the same
+// terms as project_rows_one with an L-lane instead of a 32-lane reduction, so
+// results agree to float64 rounding.
+constexpr int kGroupThreads = 256;
+
+template <typename IN, int L, int MAXF>
+__global__ void __launch_bounds__(kGroupThreads, 2)
+    project_rows_group(const IN* __restrict__ x, IN* __restrict__ out, double* __restrict__ power, size_t rows,
+                       int nt, const double2* __restrict__ vec, int k, int mode, double inv_nt) {
+  static_assert(32 % L == 0, "a lane group divides the warp");
+  extern __shared__ double2 vs[];  // [k][nt]
+  for (int i = threadIdx.x; i < k * nt; i += blockDim.x) vs[i] = vec[i];
+  __syncthreads();
+  constexpr int kGroups = kGroupThreads / L;
+  const int q = threadIdx.x % L;
+  const size_t stride = size_t(gridDim.x) * kGroups;
+  const bool subtract = mode & 1;
+  size_t row = size_t(blockIdx.x) * kGroups + threadIdx.x / L;
+  for (;; row += stride) {
+    // Every lane of a warp takes the shuffles: leave only when the warp's first row is past the end.
+    if (row - (threadIdx.x & 31) / L >= rows) break;
+    const bool live = row < rows;
+    double2 xv[MAXF];
+#pragma unroll
+    for (int f = 0; f < MAXF; ++f) {
+      const int t = q + L * f;
+      if (live && t < nt) {
+        const IN a = x[row * nt + t];
+        xv[f] = make_double2(double(a.x), double(a.y));
+      } else {
+        xv[f] = make_double2(0.0, 0.0);
+      }
+    }
+    double2 y[kProjSmall];
+    double retained = 0.0;
+#pragma unroll
+    for (int c = 0; c < kProjSmall; ++c) {
+      double yr = 0.0, yi = 0.0;
+      if (c < k) {
+#pragma unroll
+        for (int f = 0; f < MAXF; ++f) {
+          const int t = q + L * f;
+          if (t < nt) {
+            const double2 v = vs[c * nt + t];
+            yr = fma(xv[f].x, v.x, fma(-xv[f].y, v.y, yr));
+            yi = fma(xv[f].x, v.y, fma(xv[f].y, v.x, yi));
+          }
+        }
+#pragma unroll
+        for (int off = L / 2; off > 0; off >>= 1) {
+          yr += __shfl_xor_sync(0xffffffffu, yr, off);
+          yi += __shfl_xor_sync(0xffffffffu, yi, off);
+        }
+      }
+      y[c] = make_double2(yr, yi);
+      retained += yr * yr + yi * yi;
+    }
+    double pw = 0.0;
+    if (mode & 3) {
+#pragma unroll
+      for (int f = 0; f < MAXF; ++f) {
+        const int t = q + L * f;
+        if (t < nt) {
+          double2 proj = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int c = 0; c < kProjSmall; ++c) {
+            if (c < k) {  // y * conj(v)
+              const double2 v = vs[c * nt + t];
+              proj.x = fma(y[c].x, v.x, fma(y[c].y, v.y, proj.x));
+              proj.y = fma(y[c].y, v.x, fma(-y[c].x, v.y, proj.y));
+            }
+          }
+          const double2 r = subtract ? make_double2(xv[f].x - proj.x, xv[f].y - proj.y) : proj;
+          pw += r.x * r.x + r.y * r.y;
+          if ((mode & 2) && live) {
+            if constexpr (sizeof(IN) == 8)
+              reinterpret_cast<float2*>(out)[row * nt + t] = make_float2(float(r.x), float(r.y));
+            else
+              reinterpret_cast<double2*>(out)[row * nt + t] = r;
+          }
+        }
+      }
+    }
+    if (power) {
+      if (subtract) {
+#pragma unroll
+        for (int off = L / 2; off > 0; off >>= 1) pw += __shfl_xor_sync(0xffffffffu, pw, off);
+        if (q == 0 && live) power[row] = pw * inv_nt;
+      } else if (q == 0 && live) {
+        power[row] = retained * inv_nt;
+      }
+    }
+  }
+}
+
 constexpr int kRefineRows = 16;  // Casorati rows staged per block of the Rayleigh-Ritz pass
 
 // Float64 Rayleigh-Ritz matrix of the Casorati rows on m <= kRitzMax vectors:

@@ -548,9 +548,34 @@ static void launch_project(const void* iq, void* out, double* power, size_t rows
         reinterpret_cast<const double2*>(vec), int(k), mode, 1.0 / double(nt));
 }
 
+template <typename IN, int L, int MAXF = 16>
+static void launch_group(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
+                         size_t k, int mode) {
+  constexpr int kGroups = clutter::kGroupThreads / L;
+  auto kern = clutter::project_rows_group<IN, L, MAXF>;
+  const size_t smem = k * nt * sizeof(double2);
+  int dev = 0, sms = 148, per_sm = 2;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, clutter::kGroupThreads, smem);
+  const size_t want = (rows + kGroups - 1) / kGroups;
+  const size_t grid = std::min(want, size_t(sms) * size_t(per_sm > 0 ? per_sm : 1));
+  kern<<<unsigned(grid), clutter::kGroupThreads, smem>>>(static_cast<const IN*>(iq), static_cast<IN*>(out), power,
+                                                          rows, int(nt), reinterpret_cast<const double2*>(vec),
+                                                          int(k), mode, 1.0 / double(nt));
+}
+
 template <typename IN>
 static void project_dispatch(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
                              size_t k, int mode) {
+  const char* form = std::getenv("RCABEAM_PROJECT");
+  if (k <= size_t(clutter::kProjSmall) && nt <= 512 && !(form && std::string(form) == "one")) {
+    if (form && std::string(form) == "g32" && nt <= 256)
+      return launch_group<IN, 32, 8>(iq, out, power, rows, nt, vec, k, mode);
+    if (nt <= 128) return launch_group<IN, 8>(iq, out, power, rows, nt, vec, k, mode);
+    if (nt <= 256) return launch_group<IN, 16>(iq, out, power, rows, nt, vec, k, mode);
+    return launch_group<IN, 32>(iq, out, power, rows, nt, vec, k, mode);
+  }
   size_t f = (nt + 31) / 32;
   if (f <= 1) launch_project<IN, 1>(iq, out, power, rows, nt, vec, k, mode);
   else if (f <= 2) launch_project<IN, 2>(iq, out, power, rows, nt, vec, k, mode);
@@ -1375,12 +1400,12 @@ rcabeam_status rcabeam_batch_run_device(size_t n, const rcabeam_batch_ensemble* 
       {batch::run<1, 3>, batch::run<2, 3>, batch::run<3, 3>},
   };
   const Kernel kern = kernels[kind < 0 ? 0 : kind == 3 ? 3 : kind + 1][ctas_per_sm - 1];
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(batch::Smem::kBytes)) !=
-      cudaSuccess)
+  const size_t smem = kind == 3 ? batch::Smem<batch::smem_lpv<3>()>::kBytes : batch::Smem<32>::kBytes;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
     return RCABEAM_ERROR_CUDA;
   const long long want = (long long)sms * ctas_per_sm;
   const unsigned grid = unsigned(total < want ? total : want);
-  kern<<<grid, das::kThreads, batch::Smem::kBytes, st>>>(batch_queue(table, n, L, total, times));
+  kern<<<grid, das::kThreads, smem, st>>>(batch_queue(table, n, L, total, times));
   return cudaGetLastError() == cudaSuccess ? RCABEAM_SUCCESS : RCABEAM_ERROR_CUDA;
 }
 
