@@ -182,7 +182,8 @@ rcabeam_status rcabeam_opw_tc_device(const void* rc_hi, const void* rc_lo, const
  * complex128 (complex128 = 1).  Gram and basis matrices are complex128. */
 
 /* *scale (device double, zeroed by the caller) = max(|re|, |im|) over n values
- * (gpu_clutter.py:141). */
+ * (gpu_clutter.py:141); infinite for an infinite component and NaN for a NaN
+ * one, so a finite scale certifies finite input (gpu_clutter.py:36-37). */
 rcabeam_status rcabeam_clutter_scale_device(const void* iq, size_t n, int complex128, double* scale);
 
 /* Adds the upper-triangle tiles of (X / s)^H (X / s), s = *scale (1 if zero),
@@ -211,9 +212,12 @@ rcabeam_status rcabeam_heevd_device(double* gram, double* eigenvalues, size_t nt
  * mode bit 0: residual x - y V^H (else the retained part y V^H); bit 1: write
  * it to out (input dtype).  power (device double[rows], optional when writing)
  * receives |residual|^2 / nt, or sum |y|^2 / nt without bit 0 (gpu_clutter.py:196-273).
- * nt <= 512. */
+ * nt <= 512.  flags (device unsigned, optional, cleared by the caller) is ORed
+ * with 1 when an input component is not finite and with 2 when a power is not
+ * finite, the two checks gpu_clutter.py:25-40 and :271-272 make, in the same pass. */
 rcabeam_status rcabeam_project_device(const void* iq, void* out, double* power, size_t rows, size_t nt,
-                                      int complex128, const double* vectors, size_t k, int mode);
+                                      int complex128, const double* vectors, size_t k, int mode,
+                                      unsigned* flags);
 
 /* Float64 Rayleigh-Ritz matrix on complex64 rows X (extension): h (device,
  * m x m complex128, column-major; cleared inside) = (X V)^H (X V) for the m <= 16

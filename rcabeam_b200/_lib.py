@@ -41,7 +41,7 @@ SIGNATURES: dict[str, list] = {
     "rcabeam_gram_finish_device": [P, P, Z, Z],
     "rcabeam_heevd_workspace_bytes": [Z, ctypes.POINTER(c_size_t)],
     "rcabeam_heevd_device": [P, P, Z, P, Z, P],
-    "rcabeam_project_device": [P, P, P, Z, Z, I, P, Z, I],
+    "rcabeam_project_device": [P, P, P, Z, Z, I, P, Z, I, P],
     "rcabeam_ritz_matrix_device": [P, Z, Z, P, Z, P],
     "rcabeam_ensemble_static_device": [P, P, P, P, P, P, P, P, P, Z, Z, Z, Z, Z, F, F, F, F, I],
     "rcabeam_ensemble_workspace_bytes": [Z, Z, Z, ctypes.POINTER(c_size_t)],

@@ -41,7 +41,7 @@ struct Ensemble {
   int tiles, chunks;       // 64-voxel tiles x frame chunks (staged: main chunks + tail; DMAS: 32-frame chunks)
   int main_chunks;         // whole F-frame chunks
   int tma;                 // tensor maps valid (else plain staging loads)
-  int chunk_major;         // item order within the ensemble: chunk-major (1) or tile-major (0)
+  int pad;
   long long first_item;    // items before this ensemble
   long long tile_base;     // first per-tile counter of this ensemble
 };
@@ -74,16 +74,30 @@ struct Smem {
   static constexpr size_t kBytes = kAngles + size_t(kMaxAngles) * 3 * sizeof(double);
 };
 
-// KIND: the queue's one method (0 OPW, 1 XDoppler, 3 DMAS), or -1 for a mixed queue.
-template <int LPV, int KIND>
+// KIND: the queue's one method (0 OPW, 1 XDoppler, 3 DMAS), or -1 for a mixed
+// queue.  TMA: 1 when every ensemble of the queue stages by TMA, 0 when none
+// does, -1 to decide per ensemble (mixed queues); a kernel for one kind and one
+// staging carries a single producer variant.
+template <int TMA>
+__device__ __forceinline__ bool use_tma(int tma) {
+  if constexpr (TMA >= 0) return TMA == 1;
+  return tma != 0;
+}
+
+template <int LPV, int KIND, int TMA>
 __device__ __forceinline__ bool staged(const Queue& q, const das::Args& args, int method, int tma, int ei,
                                        const das::Ring& ring, const unsigned* vox, const double* angle_tab,
                                        int frame0, bool tail, uint32_t& k) {
   const int warp = threadIdx.x >> 5;
   if (warp == das::kConsumerWarps) {
     const CUtensorMap* mr = q.maps + 4 * ei + (tail ? 2 : 0);
-    if (tma) return das::produce_item<LPV, false, true>(mr, mr + 1, args, vox, angle_tab, ring, frame0, k);
-    return das::produce_item<LPV, false, false>(mr, mr + 1, args, vox, angle_tab, ring, frame0, k);
+    if constexpr (TMA != 0) {
+      if (use_tma<TMA>(tma))
+        return das::produce_item<LPV, false, true>(mr, mr + 1, args, vox, angle_tab, ring, frame0, k);
+    }
+    if constexpr (TMA != 1)
+      return das::produce_item<LPV, false, false>(mr, mr + 1, args, vox, angle_tab, ring, frame0, k);
+    return false;
   }
   if constexpr (KIND == 1) {
     return das::consume_item<LPV, false, das::kXdoppler>(args, vox, ring, frame0, warp, k);
@@ -95,39 +109,45 @@ __device__ __forceinline__ bool staged(const Queue& q, const das::Args& args, in
   }
 }
 
-template <int KIND>
+template <int KIND, int TMA>
 __device__ __forceinline__ bool staged_any(int lpv, const Queue& q, const das::Args& args, int method, int tma,
                                            int ei, const das::Ring& ring, const unsigned* vox,
                                            const double* angle_tab, int frame0, bool tail, uint32_t& k) {
   switch (lpv) {
-    case 32: return staged<32, KIND>(q, args, method, tma, ei, ring, vox, angle_tab, frame0, tail, k);
-    case 16: return staged<16, KIND>(q, args, method, tma, ei, ring, vox, angle_tab, frame0, tail, k);
-    case 8: return staged<8, KIND>(q, args, method, tma, ei, ring, vox, angle_tab, frame0, tail, k);
-    case 4: return staged<4, KIND>(q, args, method, tma, ei, ring, vox, angle_tab, frame0, tail, k);
-    default: return staged<2, KIND>(q, args, method, tma, ei, ring, vox, angle_tab, frame0, tail, k);
+    case 32: return staged<32, KIND, TMA>(q, args, method, tma, ei, ring, vox, angle_tab, frame0, tail, k);
+    case 16: return staged<16, KIND, TMA>(q, args, method, tma, ei, ring, vox, angle_tab, frame0, tail, k);
+    case 8: return staged<8, KIND, TMA>(q, args, method, tma, ei, ring, vox, angle_tab, frame0, tail, k);
+    case 4: return staged<4, KIND, TMA>(q, args, method, tma, ei, ring, vox, angle_tab, frame0, tail, k);
+    default: return staged<2, KIND, TMA>(q, args, method, tma, ei, ring, vox, angle_tab, frame0, tail, k);
   }
 }
 
 // DMAS-CCF-ACF item: 64-voxel tile x 32-frame chunk, both passes through the ring.
+template <int TMA>
 __device__ __forceinline__ bool staged_dmas(const Queue& q, const das::Args& args, int tma, int ei,
                                             const das::Ring& ring, const unsigned* vox, float* active,
                                             const double* angle_tab, int frame0, uint32_t& k) {
   const int warp = threadIdx.x >> 5;
   if (warp == das::kConsumerWarps) {
     const CUtensorMap* mr = q.maps + 4 * ei;
-    if (tma) return das::produce_dmas_item<kDmasLpv, true>(mr, mr + 1, args, vox, angle_tab, ring, frame0, k, active);
-    return das::produce_dmas_item<kDmasLpv, false>(mr, mr + 1, args, vox, angle_tab, ring, frame0, k, active);
+    if constexpr (TMA != 0) {
+      if (use_tma<TMA>(tma))
+        return das::produce_dmas_item<kDmasLpv, true>(mr, mr + 1, args, vox, angle_tab, ring, frame0, k, active);
+    }
+    if constexpr (TMA != 1)
+      return das::produce_dmas_item<kDmasLpv, false>(mr, mr + 1, args, vox, angle_tab, ring, frame0, k, active);
+    return false;
   }
   return das::consume_dmas_item<kDmasLpv>(args, vox, active, ring, frame0, warp, k);
 }
 
-// MINB resident CTAs per SM (register budget 65536 / (288 MINB)); the
-// autotuner picks the variant.  KIND as for staged().
 // Slot width of a queue of kind KIND: 32-frame slots for DMAS alone, else 64.
 template <int KIND>
 __host__ __device__ constexpr int smem_lpv() { return KIND == 3 ? kDmasLpv : 32; }
 
-template <int MINB, int KIND>
+// MINB resident CTAs per SM (register budget 65536 / (288 MINB)); the
+// autotuner picks the variant.  KIND and TMA as for staged().
+template <int MINB, int KIND, int TMA>
 __global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q) {
   using Smem = batch::Smem<smem_lpv<KIND>()>;
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -173,8 +193,7 @@ __global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q) {
     const int ei = *ens_slot;
     const Ensemble& e = q.ens[ei];
     const long long local = item - e.first_item;
-    const int tile = e.chunk_major ? int(local % e.tiles) : int(local / e.chunks);
-    const int chunk = e.chunk_major ? int(local / e.tiles) : int(local % e.chunks);
+    const int tile = int(local / e.chunks), chunk = int(local % e.chunks);
     bool ok = true;
     {
       // A private copy: the table in global memory could alias the stores of
@@ -188,14 +207,14 @@ __global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q) {
       if (KIND == 3 || (KIND < 0 && method == 3)) {
         if constexpr (KIND == 3 || KIND < 0) {
           r.slot_bytes = size_t(das::kRows) * (2 * kDmasLpv) * 8;
-          ok = staged_dmas(q, args, tma, ei, r, vox, active, angle_tab, chunk * 2 * kDmasLpv, k);
+          ok = staged_dmas<TMA>(q, args, tma, ei, r, vox, active, angle_tab, chunk * 2 * kDmasLpv, k);
         }
       } else {
         if constexpr (KIND != 3) {
           const bool tail = chunk == e.main_chunks;
           const int lpv = tail ? e.lpv_tail : e.lpv;
           r.slot_bytes = size_t(das::kRows) * (2 * lpv) * 8;
-          ok = staged_any<KIND>(lpv, q, args, method, tma, ei, r, vox, angle_tab, frame0, tail, k);
+          ok = staged_any<KIND, TMA>(lpv, q, args, method, tma, ei, r, vox, angle_tab, frame0, tail, k);
         }
       }
     }

@@ -43,15 +43,23 @@ __device__ __forceinline__ double2 load_c(const IN* p, size_t i) {
 }
 
 // Max over |re| and |im| (non-negative doubles order like their bit patterns).
+// A NaN component makes the result a quiet NaN (whose bits order above +inf
+// in the unsigned maximum), so a non-finite input always gives a non-finite
+// scale: the caller's finite-input check reads the scale instead of the input.
+constexpr unsigned long long kNanBits = 0x7ff8000000000000ull;
+
 template <typename IN>
 __global__ void max_abs_kernel(const IN* x, size_t n, unsigned long long* out) {
   double m = 0.0;
+  bool nan = false;
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
     double2 v = load_c(x, i);
     m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+    nan |= isnan(v.x) || isnan(v.y);
   }
   for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(m)));
+  const unsigned long long bits = __any_sync(0xffffffffu, nan) ? kNanBits : __double_as_longlong(m);
+  if ((threadIdx.x & 31) == 0) atomicMax(out, bits);
 }
 
 // Complex64 max |component| at HBM speed: float4 loads (two samples), four in
@@ -63,7 +71,11 @@ __global__ void __launch_bounds__(256) max_abs_c64(const float2* __restrict__ x,
   const size_t n4 = n / 2, stride = size_t(gridDim.x) * blockDim.x;
   size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   float m = 0.f;
-  auto fold = [&m](float4 v) { m = fmaxf(fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y))), fmaxf(fabsf(v.z), fabsf(v.w))); };
+  bool nan = false;
+  auto fold = [&m, &nan](float4 v) {
+    m = fmaxf(fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y))), fmaxf(fabsf(v.z), fabsf(v.w)));
+    nan |= isnan(v.x) || isnan(v.y) || isnan(v.z) || isnan(v.w);
+  };
   for (; i + 3 * stride < n4; i += 4 * stride) {
     const float4 a = __ldg(x4 + i), b = __ldg(x4 + i + stride), c = __ldg(x4 + i + 2 * stride),
                  d = __ldg(x4 + i + 3 * stride);
@@ -76,9 +88,12 @@ __global__ void __launch_bounds__(256) max_abs_c64(const float2* __restrict__ x,
   if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
     const float2 t = x[n - 1];
     m = fmaxf(m, fmaxf(fabsf(t.x), fabsf(t.y)));
+    nan |= isnan(t.x) || isnan(t.y);
   }
   for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(double(m))));
+  const unsigned long long bits =
+      __any_sync(0xffffffffu, nan) ? kNanBits : static_cast<unsigned long long>(__double_as_longlong(double(m)));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, bits);
 }
 
 // Partial Gram of one upper-triangle tile (bi <= bj) over a slice of rows.
@@ -343,40 +358,71 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-// Lane-group form of the small projection (k <= kProjSmall, nt <= L * MAXF):
-// L lanes per row (32 / L rows per warp), lane q holding frames q, q + L, ...
-// widened to float64 once, in registers, for both passes.  The k vectors are
-// staged in shared memory once per persistent CTA, so a row costs one read of
-// its samples and shared-memory broadcasts of the vectors (project_rows_one
-// reloads them through L1 for every row, twice).  The sums run over the same
-// terms as project_rows_one with an L-lane instead of a 32-lane reduction, so
-// results agree to float64 rounding.
-constexpr int kGroupThreads = 256;
+// Persistent form of the small projection (k <= kProjSmall): one warp per row,
+// lane l holding frames l, l + 32, ... widened to float64 once, in registers.
+// Each warp keeps its next kAsyncDepth - 1 rows in flight with cp.async
+// (8-byte copies for complex64, 16-byte for complex128) into a per-warp
+// shared-memory ring, so the bytes in flight per SM do not cost registers; a
+// lane reads back only the frames it copied itself, so no warp barrier is
+// needed.  The k vectors are staged in shared memory once per CTA.  Same sums
+// in the same order as project_rows_one.  flags (optional): bit 0 is set when
+// an input component is not finite, bit 1 when a row's power is not finite.
+constexpr int kAsyncThreads = 256;
+constexpr int kAsyncWarps = kAsyncThreads / 32;
+constexpr int kAsyncDepth = 3;
 
-template <typename IN, int L, int MAXF>
-__global__ void __launch_bounds__(kGroupThreads, 2)
-    project_rows_group(const IN* __restrict__ x, IN* __restrict__ out, double* __restrict__ power, size_t rows,
-                       int nt, const double2* __restrict__ vec, int k, int mode, double inv_nt) {
-  static_assert(32 % L == 0, "a lane group divides the warp");
-  extern __shared__ double2 vs[];  // [k][nt]
+__host__ __device__ inline size_t async_smem_bytes(size_t k, size_t nt, size_t elem) {
+  return (k * nt * 16 + 15) / 16 * 16 + size_t(kAsyncWarps) * kAsyncDepth * nt * elem;
+}
+
+template <typename IN>
+__device__ __forceinline__ void async_copy(IN* dst, const IN* src) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+  if constexpr (sizeof(IN) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
+template <typename IN, int MAXF>
+__global__ void __launch_bounds__(kAsyncThreads, 2)
+    project_rows_async(const IN* __restrict__ x, IN* __restrict__ out, double* __restrict__ power, size_t rows,
+                       int nt, const double2* __restrict__ vec, int k, int mode, double inv_nt,
+                       unsigned* __restrict__ flags) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double2* vs = reinterpret_cast<double2*>(smem);  // [k][nt]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  IN* ring = reinterpret_cast<IN*>(smem + (size_t(k) * nt * 16 + 15) / 16 * 16) + size_t(warp) * kAsyncDepth * nt;
   for (int i = threadIdx.x; i < k * nt; i += blockDim.x) vs[i] = vec[i];
   __syncthreads();
-  constexpr int kGroups = kGroupThreads / L;
-  const int q = threadIdx.x % L;
-  const size_t stride = size_t(gridDim.x) * kGroups;
+  const size_t stride = size_t(gridDim.x) * kAsyncWarps;
+  size_t row = size_t(blockIdx.x) * kAsyncWarps + warp;
+  auto issue = [&](size_t r, int slot) {
+    if (r < rows) {
+#pragma unroll
+      for (int f = 0; f < MAXF; ++f) {
+        const int t = lane + 32 * f;
+        if (t < nt) async_copy(ring + slot * nt + t, x + r * nt + t);
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+#pragma unroll
+  for (int d = 0; d < kAsyncDepth - 1; ++d) issue(row + d * stride, d);
   const bool subtract = mode & 1;
-  size_t row = size_t(blockIdx.x) * kGroups + threadIdx.x / L;
-  for (;; row += stride) {
-    // Every lane of a warp takes the shuffles: leave only when the warp's first row is past the end.
-    if (row - (threadIdx.x & 31) / L >= rows) break;
-    const bool live = row < rows;
+  bool bad_in = false, bad_out = false;
+  for (int i = 0; row < rows; ++i, row += stride) {
+    issue(row + (kAsyncDepth - 1) * stride, (i + kAsyncDepth - 1) % kAsyncDepth);
+    asm volatile("cp.async.wait_group %0;" ::"n"(kAsyncDepth - 1) : "memory");
+    const IN* cur = ring + (i % kAsyncDepth) * nt;
     double2 xv[MAXF];
 #pragma unroll
     for (int f = 0; f < MAXF; ++f) {
-      const int t = q + L * f;
-      if (live && t < nt) {
-        const IN a = x[row * nt + t];
+      const int t = lane + 32 * f;
+      if (t < nt) {
+        const IN a = cur[t];
         xv[f] = make_double2(double(a.x), double(a.y));
+        bad_in |= !isfinite(xv[f].x) || !isfinite(xv[f].y);
       } else {
         xv[f] = make_double2(0.0, 0.0);
       }
@@ -389,7 +435,7 @@ __global__ void __launch_bounds__(kGroupThreads, 2)
       if (c < k) {
 #pragma unroll
         for (int f = 0; f < MAXF; ++f) {
-          const int t = q + L * f;
+          const int t = lane + 32 * f;
           if (t < nt) {
             const double2 v = vs[c * nt + t];
             yr = fma(xv[f].x, v.x, fma(-xv[f].y, v.y, yr));
@@ -397,7 +443,7 @@ __global__ void __launch_bounds__(kGroupThreads, 2)
           }
         }
 #pragma unroll
-        for (int off = L / 2; off > 0; off >>= 1) {
+        for (int off = 16; off > 0; off >>= 1) {
           yr += __shfl_xor_sync(0xffffffffu, yr, off);
           yi += __shfl_xor_sync(0xffffffffu, yi, off);
         }
@@ -409,7 +455,7 @@ __global__ void __launch_bounds__(kGroupThreads, 2)
     if (mode & 3) {
 #pragma unroll
       for (int f = 0; f < MAXF; ++f) {
-        const int t = q + L * f;
+        const int t = lane + 32 * f;
         if (t < nt) {
           double2 proj = make_double2(0.0, 0.0);
 #pragma unroll
@@ -422,7 +468,7 @@ __global__ void __launch_bounds__(kGroupThreads, 2)
           }
           const double2 r = subtract ? make_double2(xv[f].x - proj.x, xv[f].y - proj.y) : proj;
           pw += r.x * r.x + r.y * r.y;
-          if ((mode & 2) && live) {
+          if (mode & 2) {
             if constexpr (sizeof(IN) == 8)
               reinterpret_cast<float2*>(out)[row * nt + t] = make_float2(float(r.x), float(r.y));
             else
@@ -434,13 +480,38 @@ __global__ void __launch_bounds__(kGroupThreads, 2)
     if (power) {
       if (subtract) {
 #pragma unroll
-        for (int off = L / 2; off > 0; off >>= 1) pw += __shfl_xor_sync(0xffffffffu, pw, off);
-        if (q == 0 && live) power[row] = pw * inv_nt;
-      } else if (q == 0 && live) {
-        power[row] = retained * inv_nt;
+        for (int off = 16; off > 0; off >>= 1) pw += __shfl_xor_sync(0xffffffffu, pw, off);
+      } else {
+        pw = retained;
+      }
+      if (lane == 0) {
+        power[row] = pw * inv_nt;
+        bad_out |= !isfinite(pw);
       }
     }
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  if (flags) {
+    const unsigned bits = (__any_sync(0xffffffffu, bad_in) ? 1u : 0u) | (__any_sync(0xffffffffu, bad_out) ? 2u : 0u);
+    if (bits && lane == 0) atomicOr(flags, bits);
+  }
+}
+
+// The flags of project_rows_async for the other projection kernels: bit 0 for
+// a non-finite input component, bit 1 for a non-finite power (when given).
+template <typename IN>
+__global__ void input_flags(const IN* __restrict__ x, size_t n, unsigned* __restrict__ flags) {
+  bool bad = false;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    bad |= !isfinite(double(x[i].x)) || !isfinite(double(x[i].y));
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flags, 1u);
+}
+
+__global__ void power_flags(const double* __restrict__ power, size_t rows, unsigned* __restrict__ flags) {
+  bool bad = false;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < rows; i += size_t(gridDim.x) * blockDim.x)
+    bad |= !isfinite(power[i]);
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flags, 2u);
 }
 
 constexpr int kRefineRows = 16;  // Casorati rows staged per block of the Rayleigh-Ritz pass

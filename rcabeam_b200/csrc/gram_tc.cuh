@@ -28,10 +28,13 @@
 // Roles (256 threads, one CTA per SM):
 //   warp 0       TMA producer: raw float32 boxes (32 columns x 16 rows;
 //                SWIZZLE_128B_ATOM_32B for TF32, SWIZZLE_128B for 3xBF16) of
-//                the unit's staged blocks into a 2-stage ring;
+//                the unit's staged blocks into the staging ring;
 //   warp 1       TMEM allocator; lane 0 issues tcgen05.mma and commits;
-//   warps 2-7    converters: staged float32 -> TF32 or BF16 hi/lo operands in
-//                the UMMA MN-major SWIZZLE_128B layout (2-stage operand ring);
+//   warps 2-7    converters: TF32 rounds the staged floats in place (the
+//                layouts coincide), so the staging ring is the operand ring
+//                and is 4 stages deep; 3xBF16 writes hi/lo operands in the
+//                UMMA MN-major SWIZZLE_128B layout (2-stage staging ring,
+//                2-stage operand ring, the same shared memory);
 //   warps 4-7    also the epilogue (TMEM lane quarters 0-3) at every flush.
 #pragma once
 
@@ -49,7 +52,7 @@ constexpr int kMaxLoads = 6;       // staged column blocks per unit
 constexpr int kMaxTasks = 4;       // output blocks per unit (4 x 128 TMEM columns)
 constexpr int kMaxUnits = 40;      // nb <= 16 blocks (T <= 1024): 136 upper blocks -> 34 units
 constexpr int kMaxBlocks = 16;
-constexpr int kRing = 2;           // staging and operand ring depth
+constexpr int kRing = 2;           // 3xBF16 staging and operand ring depth (TF32: one ring of 2 kRing)
 constexpr int kThreads = 256;
 constexpr int kConverters = 6 * 32;
 constexpr int kSlotBytes = kBlock * kRows * 4;  // 8192: one staged block per stage (f32 or bf16 hi+lo)
@@ -129,14 +132,16 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc(const __grid_constant__ C
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const Unit& u = p.units[blockIdx.x % p.nunits];
   const int slice = blockIdx.x / p.nunits;
+  // TF32: one 2 kRing-stage ring converted in place; 3xBF16: kRing staging + kRing operand stages.
+  constexpr int R = TF32 ? 2 * kRing : kRing;
   const size_t stage_bytes = size_t(p.nload_max) * kSlotBytes;
   unsigned char* staging = smem;
-  unsigned char* operands = smem + kRing * stage_bytes;
-  uint64_t* stg_full = reinterpret_cast<uint64_t*>(operands + kRing * stage_bytes);
-  uint64_t* stg_empty = stg_full + kRing;
-  uint64_t* op_full = stg_empty + kRing;
-  uint64_t* op_empty = op_full + kRing;
-  uint64_t* acc_full = op_empty + kRing;
+  unsigned char* operands = TF32 ? smem : smem + kRing * stage_bytes;
+  uint64_t* stg_full = reinterpret_cast<uint64_t*>(smem + 2 * kRing * stage_bytes);
+  uint64_t* stg_empty = stg_full + R;
+  uint64_t* op_full = stg_empty + R;
+  uint64_t* op_empty = op_full + R;
+  uint64_t* acc_full = op_empty + R;
   uint64_t* acc_empty = acc_full + 1;
   uint64_t* drain = acc_empty + 1;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
@@ -148,9 +153,9 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc(const __grid_constant__ C
   constexpr int kStagesPerFlush = kFlushRows / kRows;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kRing; ++s) {
+    for (int s = 0; s < R; ++s) {
       mbar_init(&stg_full[s], 1);
-      mbar_init(&stg_empty[s], kConverters / 32);
+      mbar_init(&stg_empty[s], TF32 ? 1 : kConverters / 32);  // TF32: freed by the MMA commit
       mbar_init(&op_full[s], kConverters / 32);
       mbar_init(&op_empty[s], 1);
     }
@@ -183,8 +188,8 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc(const __grid_constant__ C
     int k = 0;
     bool ok = true;
     for (; k < nstages && ok; ++k) {
-      const int s_ = k % kRing;
-      if (k >= kRing) ok = __all_sync(0xffffffffu, mbar_wait(&stg_empty[s_], ((k / kRing) - 1) & 1, p.err, kErrWaitEmpty));
+      const int s_ = k % R;
+      if (k >= R) ok = __all_sync(0xffffffffu, mbar_wait(&stg_empty[s_], ((k / R) - 1) & 1, p.err, kErrWaitEmpty));
       if (!ok) break;
       const int row = int(r0 + (long long)k * kRows);
       if (lane == 0) mbar_arrive_expect_tx(&stg_full[s_], uint32_t(u.nload * kSlotBytes));
@@ -198,8 +203,8 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc(const __grid_constant__ C
     }
     // Drain: the last issued stages' copies have landed before the CTA exits.
     if (lane == 0) {
-      for (int d = k - kRing < 0 ? 0 : k - kRing; d < k; ++d)
-        mbar_wait(&stg_full[d % kRing], (d / kRing) & 1, p.err, kErrWaitDrain);
+      for (int d = k - R < 0 ? 0 : k - R; d < k; ++d)
+        mbar_wait(&stg_full[d % R], (d / R) & 1, p.err, kErrWaitDrain);
     }
     __syncwarp();
   } else if (warp == 1) {
@@ -208,10 +213,10 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc(const __grid_constant__ C
       const uint32_t idesc = idesc_mn(TF32, 128, 128);
       int flushes = 0;
       for (int k = 0; k < nstages; ++k) {
-        const int s_ = k % kRing;
+        const int s_ = k % R;
         const int in_seg = k % kStagesPerFlush;
         if (in_seg == 0 && flushes > 0 && !mbar_wait(acc_empty, (flushes - 1) & 1, p.err, kErrWaitEmpty)) break;
-        if (!mbar_wait(&op_full[s_], (k / kRing) & 1, p.err, kErrWaitFull)) break;
+        if (!mbar_wait(&op_full[s_], (k / R) & 1, p.err, kErrWaitFull)) break;
         tc_fence_after();
         const uint32_t op = smem_u32(operands + s_ * stage_bytes);
         for (int t = 0; t < u.ntask; ++t) {
@@ -234,7 +239,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc(const __grid_constant__ C
             mma_f16(d, smem_desc(ah, 2048, 1024, kLayoutSw128), smem_desc(bl, 2048, 1024, kLayoutSw128), idesc, 1u);
           }
         }
-        mma_commit(&op_empty[s_]);
+        mma_commit(TF32 ? &stg_empty[s_] : &op_empty[s_]);
         if (in_seg == kStagesPerFlush - 1 || k == nstages - 1) {
           mma_commit(acc_full);
           ++flushes;
@@ -251,15 +256,15 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc(const __grid_constant__ C
     const int quarter = warp & 3;
     int flushes = 0;
     for (int k = 0; k < nstages; ++k) {
-      const int s_ = k % kRing;
-      if (!__all_sync(0xffffffffu, mbar_wait(&stg_full[s_], (k / kRing) & 1, p.err, kErrWaitFull))) break;
-      if (k >= kRing &&
-          !__all_sync(0xffffffffu, mbar_wait(&op_empty[s_], ((k / kRing) - 1) & 1, p.err, kErrWaitEmpty)))
+      const int s_ = k % R;
+      if (!__all_sync(0xffffffffu, mbar_wait(&stg_full[s_], (k / R) & 1, p.err, kErrWaitFull))) break;
+      if (!TF32 && k >= R &&
+          !__all_sync(0xffffffffu, mbar_wait(&op_empty[s_], ((k / R) - 1) & 1, p.err, kErrWaitEmpty)))
         break;
       const unsigned char* src = staging + s_ * stage_bytes;
       unsigned char* dst = operands + s_ * stage_bytes;
       if constexpr (TF32) {
-        // Same swizzled positions: an elementwise map over the staged bytes.
+        // In place (dst == src): an elementwise map over the staged bytes.
         const int chunks = u.nload * (kSlotBytes / 16);
         for (int i = ct; i < chunks; i += kConverters) {
           float4 v = reinterpret_cast<const float4*>(src)[i];
@@ -295,7 +300,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc(const __grid_constant__ C
       fence_async_smem();  // generic-proxy writes -> visible to the tensor core
       __syncwarp();
       if (lane == 0) {
-        mbar_arrive(&stg_empty[s_]);
+        if (!TF32) mbar_arrive(&stg_empty[s_]);
         mbar_arrive(&op_full[s_]);
       }
       const bool flush_here = (k % kStagesPerFlush) == kStagesPerFlush - 1 || k == nstages - 1;

@@ -548,40 +548,43 @@ static void launch_project(const void* iq, void* out, double* power, size_t rows
         reinterpret_cast<const double2*>(vec), int(k), mode, 1.0 / double(nt));
 }
 
-template <typename IN, int L, int MAXF = 16>
-static void launch_group(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
-                         size_t k, int mode) {
-  constexpr int kGroups = clutter::kGroupThreads / L;
-  auto kern = clutter::project_rows_group<IN, L, MAXF>;
-  const size_t smem = k * nt * sizeof(double2);
+template <typename IN, int MAXF>
+static bool launch_async(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
+                         size_t k, int mode, unsigned* flags) {
+  auto kern = clutter::project_rows_async<IN, MAXF>;
+  const size_t smem = clutter::async_smem_bytes(k, nt, sizeof(IN));
+  if (smem > 110 * 1024) return false;  // keep two CTAs per SM
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+    return false;
   int dev = 0, sms = 148, per_sm = 2;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, clutter::kGroupThreads, smem);
-  const size_t want = (rows + kGroups - 1) / kGroups;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, clutter::kAsyncThreads, smem);
+  const size_t want = (rows + clutter::kAsyncWarps - 1) / clutter::kAsyncWarps;
   const size_t grid = std::min(want, size_t(sms) * size_t(per_sm > 0 ? per_sm : 1));
-  kern<<<unsigned(grid), clutter::kGroupThreads, smem>>>(static_cast<const IN*>(iq), static_cast<IN*>(out), power,
+  kern<<<unsigned(grid), clutter::kAsyncThreads, smem>>>(static_cast<const IN*>(iq), static_cast<IN*>(out), power,
                                                           rows, int(nt), reinterpret_cast<const double2*>(vec),
-                                                          int(k), mode, 1.0 / double(nt));
+                                                          int(k), mode, 1.0 / double(nt), flags);
+  return true;
 }
 
 template <typename IN>
 static void project_dispatch(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
-                             size_t k, int mode) {
+                             size_t k, int mode, unsigned* flags) {
   const char* form = std::getenv("RCABEAM_PROJECT");
-  if (k <= size_t(clutter::kProjSmall) && nt <= 512 && !(form && std::string(form) == "one")) {
-    if (form && std::string(form) == "g32" && nt <= 256)
-      return launch_group<IN, 32, 8>(iq, out, power, rows, nt, vec, k, mode);
-    if (nt <= 128) return launch_group<IN, 8>(iq, out, power, rows, nt, vec, k, mode);
-    if (nt <= 256) return launch_group<IN, 16>(iq, out, power, rows, nt, vec, k, mode);
-    return launch_group<IN, 32>(iq, out, power, rows, nt, vec, k, mode);
+  if (k <= size_t(clutter::kProjSmall) && !(form && std::string(form) == "one")) {
+    if (nt <= 256 && launch_async<IN, 8>(iq, out, power, rows, nt, vec, k, mode, flags)) return;
+    if (nt > 256 && launch_async<IN, 16>(iq, out, power, rows, nt, vec, k, mode, flags)) return;
   }
+  if (flags) clutter::input_flags<IN><<<296, 256>>>(static_cast<const IN*>(iq), rows * nt, flags);
   size_t f = (nt + 31) / 32;
   if (f <= 1) launch_project<IN, 1>(iq, out, power, rows, nt, vec, k, mode);
   else if (f <= 2) launch_project<IN, 2>(iq, out, power, rows, nt, vec, k, mode);
   else if (f <= 4) launch_project<IN, 4>(iq, out, power, rows, nt, vec, k, mode);
   else if (f <= 8) launch_project<IN, 8>(iq, out, power, rows, nt, vec, k, mode);
   else launch_project<IN, 16>(iq, out, power, rows, nt, vec, k, mode);
+  if (flags && power) clutter::power_flags<<<148, 256>>>(power, rows, flags);
 }
 
 // ---------------------------------------------- no-allocation entry point --
@@ -822,14 +825,14 @@ rcabeam_status rcabeam_heevd_device(double* gram, double* eigenvalues, size_t nt
 }
 
 rcabeam_status rcabeam_project_device(const void* iq, void* out, double* power, size_t rows, size_t nt,
-                                      int complex128, const double* vectors, size_t k, int mode) {
+                                      int complex128, const double* vectors, size_t k, int mode, unsigned* flags) {
   if (!iq || !rows || !nt || nt > 512 || (k && !vectors) || mode < 0 || mode > 3 || ((mode & 2) && !out) ||
       (!power && !(mode & 2)))
     return RCABEAM_ERROR_ARGUMENT;
   if (complex128)
-    project_dispatch<double2>(iq, out, power, rows, nt, vectors, k, mode);
+    project_dispatch<double2>(iq, out, power, rows, nt, vectors, k, mode, flags);
   else
-    project_dispatch<float2>(iq, out, power, rows, nt, vectors, k, mode);
+    project_dispatch<float2>(iq, out, power, rows, nt, vectors, k, mode, flags);
   return launch_status();
 }
 
@@ -1271,10 +1274,6 @@ bool batch_plan(size_t n, const rcabeam_batch_ensemble* list, std::vector<batch:
       e.lpv_tail = tail ? int(std::max(pow2_at_least(tail), 4u) / 2) : 0;
       e.chunks = e.main_chunks + (tail ? 1 : 0);
     }
-    {
-      const char* order = std::getenv("RCABEAM_BATCH_ORDER");
-      e.chunk_major = order && std::string(order) == "chunk" ? 1 : 0;
-    }
     e.tma = (d.nt * 8) % 16 == 0 && reinterpret_cast<uintptr_t>(d.rc) % 16 == 0 &&
             reinterpret_cast<uintptr_t>(d.cr) % 16 == 0 && encode_fn() != nullptr;
     e.first_item = items;
@@ -1359,7 +1358,7 @@ rcabeam_status rcabeam_batch_prepare(size_t n, const rcabeam_batch_ensemble* lis
       if (!frames) continue;
       if (!make_slab_map(&maps[4 * i + 2 * part], e.args.rc, 8, nt, ns, slabs, frames, das::kRows) ||
           !make_slab_map(&maps[4 * i + 2 * part + 1], e.args.cr, 8, nt, ns, slabs, frames, das::kRows))
-        e.tma = 0;
+        return RCABEAM_ERROR_ARGUMENT;  // the run's kernel variant follows the plan's tma flags
     }
   }
   unsigned char* t = static_cast<unsigned char*>(table);
@@ -1388,19 +1387,26 @@ rcabeam_status rcabeam_batch_run_device(size_t n, const rcabeam_batch_ensemble* 
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  // A queue of one method runs the kernel compiled for that method alone.
-  int kind = list[0].method;
-  for (size_t i = 1; i < n; ++i)
+  // A queue of one method whose ensembles all stage the same way (TMA or plain
+  // loads) at two or three CTAs per SM runs the kernel compiled for that
+  // method and staging alone; anything else runs the general kernel.
+  std::vector<batch::Ensemble> ens;
+  batch_plan(n, list, &ens, &L, &total);
+  int kind = list[0].method, tma = ens[0].tma;
+  for (size_t i = 1; i < n; ++i) {
     if (list[i].method != kind) kind = -1;
+    if (ens[i].tma != tma) tma = -1;
+  }
   using Kernel = void (*)(const batch::Queue);
-  static const Kernel kernels[4][3] = {
-      {batch::run<1, -1>, batch::run<2, -1>, batch::run<3, -1>},
-      {batch::run<1, 0>, batch::run<2, 0>, batch::run<3, 0>},
-      {batch::run<1, 1>, batch::run<2, 1>, batch::run<3, 1>},
-      {batch::run<1, 3>, batch::run<2, 3>, batch::run<3, 3>},
+  static const Kernel general[3] = {batch::run<1, -1, -1>, batch::run<2, -1, -1>, batch::run<3, -1, -1>};
+  static const Kernel special[3][2][2] = {  // [kind][tma][ctas_per_sm - 2]
+      {{batch::run<2, 0, 0>, batch::run<3, 0, 0>}, {batch::run<2, 0, 1>, batch::run<3, 0, 1>}},
+      {{batch::run<2, 1, 0>, batch::run<3, 1, 0>}, {batch::run<2, 1, 1>, batch::run<3, 1, 1>}},
+      {{batch::run<2, 3, 0>, batch::run<3, 3, 0>}, {batch::run<2, 3, 1>, batch::run<3, 3, 1>}},
   };
-  const Kernel kern = kernels[kind < 0 ? 0 : kind == 3 ? 3 : kind + 1][ctas_per_sm - 1];
-  const size_t smem = kind == 3 ? batch::Smem<batch::smem_lpv<3>()>::kBytes : batch::Smem<32>::kBytes;
+  const bool specific = kind >= 0 && tma >= 0 && ctas_per_sm >= 2;
+  const Kernel kern = specific ? special[kind == 3 ? 2 : kind][tma][ctas_per_sm - 2] : general[ctas_per_sm - 1];
+  const size_t smem = specific && kind == 3 ? batch::Smem<batch::smem_lpv<3>()>::kBytes : batch::Smem<32>::kBytes;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
     return RCABEAM_ERROR_CUDA;
   const long long want = (long long)sms * ctas_per_sm;

@@ -35,7 +35,10 @@ _GRAM_PRECISION = {"complex128": 0, "complex64": 1, "tf32": 2, "bf16x3": 3}
 _GRAM_EPS = {"complex128": 2.0 ** -52, "complex64": 2.0 ** -23, "tf32": 2.0 ** -10, "bf16x3": 2.0 ** -16}
 
 
-def _inputs(iq) -> tuple[torch.Tensor, ...]:
+def _inputs(iq, *, check_finite: bool = True) -> tuple[torch.Tensor, ...]:
+    """The reference's input checks (gpu_clutter.py:25-40).  Callers whose kernel
+    flags non-finite samples itself pass check_finite=False and raise the same
+    error from the flag, which saves a separate pass over the input."""
     arrays = iq if isinstance(iq, tuple) else (iq,)
     if not arrays:
         raise ValueError("At least one IQ array is required")
@@ -46,7 +49,7 @@ def _inputs(iq) -> tuple[torch.Tensor, ...]:
             raise ValueError("IQ must be nonempty with frames on the last axis")
         if a.device.index != torch.cuda.current_device():
             raise ValueError("IQ must be on the current CUDA device")
-        if not bool(torch.isfinite(torch.view_as_real(a)).all()):
+        if check_finite and not bool(torch.isfinite(torch.view_as_real(a)).all()):
             raise ValueError("IQ must be finite")
     if any(a.shape[-1] != arrays[0].shape[-1] for a in arrays):
         raise ValueError("All IQ arrays must share the frame count")
@@ -129,7 +132,9 @@ def temporal_basis(iq, *, method: str = "gram", precision: str = "complex128", t
     A tuple of arrays estimates one shared basis over all of their rows; with a
     torch.distributed process group, over the rows of every rank of the group.
     """
-    arrays = _inputs(iq)
+    # Without a group the Casorati scale pass certifies finite input (a non-finite
+    # component gives a non-finite scale), so the input is read once less.
+    arrays = _inputs(iq, check_finite=group is not None)
     frames = arrays[0].shape[-1]
     if precision not in _GRAM_PRECISION:
         raise ValueError("Precision must be complex64, complex128, tf32 or bf16x3")
@@ -138,6 +143,8 @@ def temporal_basis(iq, *, method: str = "gram", precision: str = "complex128", t
     begin = perf_counter()
     gram = Gram(frames, arrays[0].device)
     rows = gram.accumulate(arrays, precision, group)
+    if not np.isfinite(float(gram.scale.item())):
+        raise ValueError("IQ must be finite")
     matrix = torch.view_as_real(gram.vectors())
     if not bool(torch.isfinite(matrix).all()):
         raise np.linalg.LinAlgError("Nonfinite Gram matrix; rescale the IQ input")
@@ -192,10 +199,10 @@ def _filter_vectors(basis, frames: int, start: int, stop: int) -> tuple[torch.Te
 
 
 def _project(matrix: torch.Tensor, vectors_cm: torch.Tensor, k: int, mode: int, out: torch.Tensor | None,
-             power: torch.Tensor | None) -> None:
+             power: torch.Tensor | None, flags: torch.Tensor | None = None) -> None:
     _lib.call("rcabeam_project_device", matrix.data_ptr(), None if out is None else out.data_ptr(),
               None if power is None else power.data_ptr(), matrix.shape[0], matrix.shape[1], _is128(matrix),
-              vectors_cm.data_ptr() if k else None, k, mode)
+              vectors_cm.data_ptr() if k else None, k, mode, None if flags is None else flags.data_ptr())
 
 
 def apply_temporal_filter(iq, basis, *, rank_start: int, rank_stop: int | None = None):
@@ -220,16 +227,21 @@ def filtered_power(iq, basis, *, rank_start: int, rank_stop: int | None = None) 
     """Float64 filtered power without materializing filtered IQ (gpu_clutter.py:244-273)."""
     if not isinstance(iq, torch.Tensor):
         raise ValueError("Power requires one coherent beamformed IQ array")
-    arrays = _inputs(iq)
+    arrays = _inputs(iq, check_finite=False)  # the projection flags non-finite samples
     frames = arrays[0].shape[-1]
     start, stop = _rank_interval(frames, rank_start, rank_stop)
     vectors, subtract = _filter_vectors(basis, frames, start, stop)
     if start == stop:
+        _inputs(iq)
         return torch.zeros(iq.shape[:-1], dtype=torch.float64, device=iq.device)
     m = _rows(iq)
     power = torch.empty(m.shape[0], dtype=torch.float64, device=iq.device)
-    _project(m, vectors, vectors.shape[0], 1 if subtract else 0, None, power)
-    if not bool(torch.isfinite(power).all()):
+    flags = torch.zeros(1, dtype=torch.int32, device=iq.device)
+    _project(m, vectors, vectors.shape[0], 1 if subtract else 0, None, power, flags)
+    bits = int(flags.item())
+    if bits & 1:
+        raise ValueError("IQ must be finite")
+    if bits & 2:
         raise np.linalg.LinAlgError("Nonfinite filtered power; rescale the input")
     return power.reshape(iq.shape[:-1])
 

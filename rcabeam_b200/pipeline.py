@@ -167,7 +167,7 @@ class FilteredOpw:
             if self.refine:
                 self._refine()
             _lib.call("rcabeam_project_device", self.iq.data_ptr(), None, self.power.data_ptr(), self.nv,
-                      self.channel_shape[3], 0, self.vectors.data_ptr(), self.k, 1 if self.subtract else 0)
+                      self.channel_shape[3], 0, self.vectors.data_ptr(), self.k, 1 if self.subtract else 0, None)
         ev[5].record()
         self.last_das_event_ms = (ev[1], ev[2])
         return self.power.view(self.shape)
@@ -186,7 +186,7 @@ class FilteredOpw:
             self._select_vectors()
             for src, dst in zip((rc, cr), self.filtered):
                 _lib.call("rcabeam_project_device", src.data_ptr(), dst.data_ptr(), None, rows, nt, 0,
-                          self.vectors.data_ptr(), self.k, (1 if self.subtract else 0) | 2)
+                          self.vectors.data_ptr(), self.k, (1 if self.subtract else 0) | 2, None)
         ev[3].record()
         if after_inputs is not None:
             after_inputs()

@@ -275,8 +275,10 @@ def test_projection_rows_match_float64(rows, nt, k, mode, offset):
     vec = _dev(np.asfortranarray(q).ravel(order="F"))
     out = torch.zeros(rows * nt, dtype=torch.complex64, device="cuda") if mode & 2 else None
     power = torch.zeros(rows, dtype=torch.float64, device="cuda")
+    flags = torch.zeros(1, dtype=torch.int32, device="cuda")
     _lib.call("rcabeam_project_device", iq.data_ptr(), None if out is None else out.data_ptr(), power.data_ptr(),
-              rows, nt, 0, vec.data_ptr(), k, mode)
+              rows, nt, 0, vec.data_ptr(), k, mode, flags.data_ptr())
+    assert int(flags.item()) == 0
     x = host.astype(np.complex128)
     y = x @ q
     part = y @ q.conj().T
@@ -332,3 +334,47 @@ def test_ritz_refinement_is_the_float64_ritz_step():
     p64 = proj(b64[:, :k])
     err = lambda b: torch.linalg.matrix_norm(proj(b) - p64).item()  # noqa: E731
     assert err(refined) <= err(b16[:, :k]) * (1 + 1e-6)
+
+
+@pytest.mark.parametrize("dtype", [torch.complex64, torch.complex128])
+@pytest.mark.parametrize("k,nt", [(3, 64), (3, 400), (6, 64)])
+def test_projection_flags_non_finite_input_and_power(dtype, k, nt):
+    """The projection's flags word: bit 0 for a NaN or infinite input component (both the
+    persistent kernel, k <= 4, and the general one), bit 1 for an overflowing power."""
+    rows = 1000
+    gen = torch.Generator(device="cuda").manual_seed(k + nt)
+    x = torch.randn((rows, nt), dtype=dtype, device="cuda", generator=gen)
+    q, _ = torch.linalg.qr(torch.randn((nt, k), dtype=torch.complex128, device="cuda", generator=gen))
+    vec = q.transpose(0, 1).contiguous()  # column-major (nt x k)
+    power = torch.empty(rows, dtype=torch.float64, device="cuda")
+
+    def flags_of(a):
+        flags = torch.zeros(1, dtype=torch.int32, device="cuda")
+        _lib.call("rcabeam_project_device", a.data_ptr(), None, power.data_ptr(), rows, nt,
+                  int(a.dtype == torch.complex128), vec.data_ptr(), k, 1, flags.data_ptr())
+        return int(flags.item())
+
+    assert flags_of(x) == 0
+    for bad in (complex(float("nan"), 0.0), complex(0.0, float("inf"))):
+        y = x.clone()
+        y[517, nt // 3] = bad
+        assert flags_of(y) & 1
+    if dtype == torch.complex128:
+        assert flags_of(x * 1e200) == 2  # finite input, |x|^2 overflows
+
+
+def test_filtered_power_and_basis_reject_non_finite_input():
+    """filtered_power and temporal_basis raise the reference's ValueError for NaN / infinite IQ
+    (gpu_clutter.py:36-37) from the projection flags and the Casorati scale."""
+    iq = torch.randn((300, 16), dtype=torch.complex64, device="cuda")
+    _, basis = gpu_clutter.temporal_basis(iq)
+    for bad in (complex(float("nan"), 1.0), complex(float("-inf"), 0.0)):
+        y = iq.clone()
+        y[123, 7] = bad
+        with pytest.raises(ValueError, match="finite"):
+            gpu_clutter.filtered_power(y, basis, rank_start=2)
+        with pytest.raises(ValueError, match="finite"):
+            gpu_clutter.filtered_power(y, basis, rank_start=2, rank_stop=2)
+        for precision in ("complex128", "bf16x3"):
+            with pytest.raises(ValueError, match="finite"):
+                gpu_clutter.temporal_basis(y, precision=precision)
