@@ -141,14 +141,27 @@ __device__ __forceinline__ bool staged_dmas(const Queue& q, const das::Args& arg
   return das::consume_dmas_item<kDmasLpv>(args, vox, active, ring, frame0, warp, k);
 }
 
+// Per-ensemble arguments of a short queue, passed in the kernel's parameter
+// space: the DMAS producer's float64 delay chain reads the geometry constants
+// at every step, and from the parameter space they are constant-bank loads the
+// compiler may hoist or repeat at will, where a copy from the global table
+// competes for the 72-register budget (measured: 41 % more instructions for a
+// DMAS ensemble through the table than through the single-ensemble kernel).
+constexpr int kParamEnsembles = 48;  // 48 x 160 B of kernel parameters
+struct ParamArgs {
+  das::Args args[kParamEnsembles];
+};
+
 // Slot width of a queue of kind KIND: 32-frame slots for DMAS alone, else 64.
 template <int KIND>
 __host__ __device__ constexpr int smem_lpv() { return KIND == 3 ? kDmasLpv : 32; }
 
 // MINB resident CTAs per SM (register budget 65536 / (288 MINB)); the
 // autotuner picks the variant.  KIND and TMA as for staged().
+// The DMAS kernel (KIND 3) takes every ensemble's arguments from pa (queues of
+// at most kParamEnsembles); the others read the table.
 template <int MINB, int KIND, int TMA>
-__global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q) {
+__global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q, const __grid_constant__ ParamArgs pa) {
   using Smem = batch::Smem<smem_lpv<KIND>()>;
   extern __shared__ __align__(1024) unsigned char smem[];
   const das::Ring ring{smem + Smem::kData, 0, reinterpret_cast<das::StageTap*>(smem + Smem::kTaps),
@@ -195,11 +208,8 @@ __global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q) {
     const long long local = item - e.first_item;
     const int tile = int(local / e.chunks), chunk = int(local % e.chunks);
     bool ok = true;
-    {
-      // A private copy: the table in global memory could alias the stores of
-      // the item, so its fields would be reloaded inside the hot loops.
-      const das::Args args = e.args;
-      const int method = e.method, tma = e.tma;
+    const int method = e.method, tma = e.tma;
+    auto item_body = [&](const das::Args& args) {
       das::load_item_tables(args, size_t(tile) * das::kTileVoxels, vox, angle_tab);
       __syncthreads();
       das::Ring r = ring;
@@ -217,6 +227,15 @@ __global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q) {
           ok = staged_any<KIND, TMA>(lpv, q, args, method, tma, ei, r, vox, angle_tab, frame0, tail, k);
         }
       }
+    };
+    if constexpr (KIND == 3) {
+      item_body(pa.args[ei]);
+    } else {
+      // The other kernels take a private copy: the table in global memory
+      // could alias the item's stores, so its fields would be reloaded inside
+      // the hot loops.  (From the parameter space the OPW kernel spills.)
+      const das::Args local = e.args;
+      item_body(local);
     }
     if (!ok && lane == 0) atomicExch(fail, 1);
     __syncthreads();  // every warp's results of this item are issued

@@ -497,6 +497,119 @@ __global__ void __launch_bounds__(kAsyncThreads, 2)
   }
 }
 
+// Register form of project_rows_async for complex64 rows, K <= 3 vectors and
+// nt <= 32 F: lane l holds the vectors' values at its frames l, l + 32, ...
+// in registers for the whole launch, so a row costs its samples' read and
+// float64 arithmetic only (the shared-memory form reads 2 K F double2 per
+// lane and row back, about twice the shared-memory cycles its float64 work
+// takes).  Same sums in the same order as project_rows_async.
+constexpr int kRegThreads = 128;
+constexpr int kRegWarps = kRegThreads / 32;
+
+template <int F, int K>
+__global__ void __launch_bounds__(kRegThreads, 3)
+    project_rows_reg(const float2* __restrict__ x, float2* __restrict__ out, double* __restrict__ power,
+                     size_t rows, int nt, const double2* __restrict__ vec, int mode, double inv_nt,
+                     unsigned* __restrict__ flags) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* ring = reinterpret_cast<float2*>(smem) + size_t(warp) * kAsyncDepth * nt;
+  double2 v[K][F];
+#pragma unroll
+  for (int c = 0; c < K; ++c)
+#pragma unroll
+    for (int f = 0; f < F; ++f) {
+      const int t = lane + 32 * f;
+      v[c][f] = t < nt ? vec[c * nt + t] : make_double2(0.0, 0.0);
+    }
+  const size_t stride = size_t(gridDim.x) * kRegWarps;
+  size_t row = size_t(blockIdx.x) * kRegWarps + warp;
+  auto issue = [&](size_t r, int slot) {
+    if (r < rows) {
+#pragma unroll
+      for (int f = 0; f < F; ++f) {
+        const int t = lane + 32 * f;
+        if (t < nt) async_copy(ring + slot * nt + t, x + r * nt + t);
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+#pragma unroll
+  for (int d = 0; d < kAsyncDepth - 1; ++d) issue(row + d * stride, d);
+  const bool subtract = mode & 1;
+  bool bad_in = false, bad_out = false;
+  for (int i = 0; row < rows; ++i, row += stride) {
+    issue(row + (kAsyncDepth - 1) * stride, (i + kAsyncDepth - 1) % kAsyncDepth);
+    asm volatile("cp.async.wait_group %0;" ::"n"(kAsyncDepth - 1) : "memory");
+    const float2* cur = ring + (i % kAsyncDepth) * nt;
+    double2 xv[F];
+#pragma unroll
+    for (int f = 0; f < F; ++f) {
+      const int t = lane + 32 * f;
+      if (t < nt) {
+        const float2 a = cur[t];
+        xv[f] = make_double2(double(a.x), double(a.y));
+        bad_in |= !isfinite(a.x) || !isfinite(a.y);
+      } else {
+        xv[f] = make_double2(0.0, 0.0);
+      }
+    }
+    double2 y[K];
+    double retained = 0.0;
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+      double yr = 0.0, yi = 0.0;
+#pragma unroll
+      for (int f = 0; f < F; ++f) {
+        yr = fma(xv[f].x, v[c][f].x, fma(-xv[f].y, v[c][f].y, yr));
+        yi = fma(xv[f].x, v[c][f].y, fma(xv[f].y, v[c][f].x, yi));
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        yr += __shfl_xor_sync(0xffffffffu, yr, off);
+        yi += __shfl_xor_sync(0xffffffffu, yi, off);
+      }
+      y[c] = make_double2(yr, yi);
+      retained += yr * yr + yi * yi;
+    }
+    double pw = 0.0;
+    if (mode & 3) {
+#pragma unroll
+      for (int f = 0; f < F; ++f) {
+        const int t = lane + 32 * f;
+        if (t < nt) {
+          double2 proj = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int c = 0; c < K; ++c) {  // y * conj(v)
+            proj.x = fma(y[c].x, v[c][f].x, fma(y[c].y, v[c][f].y, proj.x));
+            proj.y = fma(y[c].y, v[c][f].x, fma(-y[c].x, v[c][f].y, proj.y));
+          }
+          const double2 r = subtract ? make_double2(xv[f].x - proj.x, xv[f].y - proj.y) : proj;
+          pw += r.x * r.x + r.y * r.y;
+          if (mode & 2) out[row * nt + t] = make_float2(float(r.x), float(r.y));
+        }
+      }
+    }
+    if (power) {
+      if (subtract) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) pw += __shfl_xor_sync(0xffffffffu, pw, off);
+      } else {
+        pw = retained;
+      }
+      if (lane == 0) {
+        power[row] = pw * inv_nt;
+        bad_out |= !isfinite(pw);
+      }
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  if (flags) {
+    const unsigned bits = (__any_sync(0xffffffffu, bad_in) ? 1u : 0u) | (__any_sync(0xffffffffu, bad_out) ? 2u : 0u);
+    if (bits && lane == 0) atomicOr(flags, bits);
+  }
+}
+
 // The flags of project_rows_async for the other projection kernels: bit 0 for
 // a non-finite input component, bit 1 for a non-finite power (when given).
 template <typename IN>

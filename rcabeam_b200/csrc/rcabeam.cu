@@ -569,10 +569,45 @@ static bool launch_async(const void* iq, void* out, double* power, size_t rows, 
   return true;
 }
 
+template <int F, int K>
+static void launch_reg(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
+                       int mode, unsigned* flags) {
+  auto kern = clutter::project_rows_reg<F, K>;
+  const size_t smem = size_t(clutter::kRegWarps) * clutter::kAsyncDepth * nt * sizeof(float2);
+  int dev = 0, sms = 148, per_sm = 3;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, clutter::kRegThreads, smem);
+  const size_t want = (rows + clutter::kRegWarps - 1) / clutter::kRegWarps;
+  const size_t grid = std::min(want, size_t(sms) * size_t(per_sm > 0 ? per_sm : 1));
+  kern<<<unsigned(grid), clutter::kRegThreads, smem>>>(static_cast<const float2*>(iq), static_cast<float2*>(out),
+                                                        power, rows, int(nt), reinterpret_cast<const double2*>(vec),
+                                                        mode, 1.0 / double(nt), flags);
+}
+
+// Complex64, 1-3 vectors, 33-256 frames: the register form.
+static bool project_reg(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
+                        size_t k, int mode, unsigned* flags) {
+  if (k < 1 || k > 3 || nt <= 32 || nt > 256) return false;
+  const int f = int((nt + 31) / 32);
+  using Launch = void (*)(const void*, void*, double*, size_t, size_t, const double*, int, unsigned*);
+  static const Launch table[3][3] = {  // [k - 1][F = 4, 7, 8]
+      {launch_reg<4, 1>, launch_reg<7, 1>, launch_reg<8, 1>},
+      {launch_reg<4, 2>, launch_reg<7, 2>, launch_reg<8, 2>},
+      {launch_reg<4, 3>, launch_reg<7, 3>, launch_reg<8, 3>},
+  };
+  table[k - 1][f <= 4 ? 0 : f <= 7 ? 1 : 2](iq, out, power, rows, nt, vec, mode, flags);
+  return true;
+}
+
 template <typename IN>
 static void project_dispatch(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
                              size_t k, int mode, unsigned* flags) {
   const char* form = std::getenv("RCABEAM_PROJECT");
+  const bool reg_off = form && (std::string(form) == "one" || std::string(form) == "async");
+  if constexpr (sizeof(IN) == 8) {
+    if (!reg_off && project_reg(iq, out, power, rows, nt, vec, k, mode, flags)) return;
+  }
   if (k <= size_t(clutter::kProjSmall) && !(form && std::string(form) == "one")) {
     if (nt <= 256 && launch_async<IN, 8>(iq, out, power, rows, nt, vec, k, mode, flags)) return;
     if (nt > 256 && launch_async<IN, 16>(iq, out, power, rows, nt, vec, k, mode, flags)) return;
@@ -1397,21 +1432,27 @@ rcabeam_status rcabeam_batch_run_device(size_t n, const rcabeam_batch_ensemble* 
     if (list[i].method != kind) kind = -1;
     if (ens[i].tma != tma) tma = -1;
   }
-  using Kernel = void (*)(const batch::Queue);
+  using Kernel = void (*)(const batch::Queue, const batch::ParamArgs);
   static const Kernel general[3] = {batch::run<1, -1, -1>, batch::run<2, -1, -1>, batch::run<3, -1, -1>};
   static const Kernel special[3][2][2] = {  // [kind][tma][ctas_per_sm - 2]
       {{batch::run<2, 0, 0>, batch::run<3, 0, 0>}, {batch::run<2, 0, 1>, batch::run<3, 0, 1>}},
       {{batch::run<2, 1, 0>, batch::run<3, 1, 0>}, {batch::run<2, 1, 1>, batch::run<3, 1, 1>}},
       {{batch::run<2, 3, 0>, batch::run<3, 3, 0>}, {batch::run<2, 3, 1>, batch::run<3, 3, 1>}},
   };
-  const bool specific = kind >= 0 && tma >= 0 && ctas_per_sm >= 2;
+  const bool specific = kind >= 0 && tma >= 0 && ctas_per_sm >= 2 && (kind != 3 || n <= size_t(batch::kParamEnsembles));
   const Kernel kern = specific ? special[kind == 3 ? 2 : kind][tma][ctas_per_sm - 2] : general[ctas_per_sm - 1];
   const size_t smem = specific && kind == 3 ? batch::Smem<batch::smem_lpv<3>()>::kBytes : batch::Smem<32>::kBytes;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
     return RCABEAM_ERROR_CUDA;
   const long long want = (long long)sms * ctas_per_sm;
   const unsigned grid = unsigned(total < want ? total : want);
-  kern<<<grid, das::kThreads, smem, st>>>(batch_queue(table, n, L, total, times));
+  static batch::ParamArgs pa;  // host staging of the launch's parameters (copied at launch)
+  static std::mutex pa_lock;
+  std::lock_guard<std::mutex> guard(pa_lock);
+  pa = batch::ParamArgs{};
+  if (specific && kind == 3)
+    for (size_t i = 0; i < n; ++i) pa.args[i] = ens[i].args;
+  kern<<<grid, das::kThreads, smem, st>>>(batch_queue(table, n, L, total, times), pa);
   return cudaGetLastError() == cudaSuccess ? RCABEAM_SUCCESS : RCABEAM_ERROR_CUDA;
 }
 
