@@ -441,7 +441,11 @@ def run_batching(args) -> dict:
                                             "p99": round(float(np.percentile(seq_done, 99)), 1)}},
         "power_rel_l2_batch_vs_sequential_max": worst,
         "autotune": {**choice, "seconds": round(tune_s, 2)},
-        "launches": "one persistent kernel per method (own register budget), forked streams, one CUDA graph",
+        "launches": "per method either one persistent kernel (own register budget) or the single-ensemble "
+                    "kernels launched per ensemble, as the autotuner measured faster; forked streams, one CUDA graph",
+        "mode_by_method": {p.ensembles[0].method: ("per-ensemble grids" if p.ctas_per_sm == 0
+                                                   else f"persistent, {p.ctas_per_sm} CTAs/SM")
+                           for p in queue.parts},
         "latency_definition": "completion time since the queue started (device global timer for the persistent "
                               "kernel, CUDA events for sequential launches)",
         "dtype": "f32 math on c64 packed IQ (float64 geometry)", "data": "synthetic seeded complex Gaussian channels",
@@ -449,7 +453,7 @@ def run_batching(args) -> dict:
                                "(central block of the 128-wide grid), frames {50,100,200,400}, 128 ch, "
                                "angles {5,7,11}, ns 512, 50% OPW / 25% XDoppler / 25% DMAS-CCF-ACF",
                    "seed": args.seed, "ensembles": shapes},
-        "clocks": clocks, "gpu_launches": steps * len(queue.parts),
+        "clocks": clocks, "gpu_launches": steps * sum(p.kernel_launches() for p in queue.parts),
     }
 
 

@@ -318,7 +318,9 @@ rcabeam_status rcabeam_batch_prepare(size_t n, const rcabeam_batch_ensemble* lis
 
 /* Enqueues on `stream` (a cudaStream_t; capturable into a CUDA graph): clears
  * the counters and every pd, then runs the persistent kernel with ctas_per_sm
- * (1-3) CTAs per SM (a queue of one method runs that method's own kernel).  times (device, n + 1 uint64): kernel start, then each
+ * (1-3) CTAs per SM (a queue of one method runs that method's own kernel), or
+ * with ctas_per_sm = 0 launches every ensemble through the single-ensemble
+ * kernels in queue order.  times (device, n + 1 uint64): start, then each
  * ensemble's completion, in global-timer nanoseconds. */
 rcabeam_status rcabeam_batch_run_device(size_t n, const rcabeam_batch_ensemble* list, void* table,
                                         size_t table_bytes, unsigned long long* times, int ctas_per_sm,

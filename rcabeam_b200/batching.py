@@ -122,7 +122,9 @@ class Ensemble:
 
 
 class _SubQueue:
-    """The ensembles of one method: device table, completion times, register budget."""
+    """The ensembles of one method: device table, completion times, and how it runs:
+    ``ctas_per_sm`` 1-3 is the persistent kernel at that many CTAs per SM, 0 the
+    single-ensemble kernels launched per ensemble on the sub-queue's stream."""
 
     def __init__(self, lib, indices, ensembles, ctas_per_sm: int, voxel_limit: int | None, device):
         self.lib = lib
@@ -139,6 +141,20 @@ class _SubQueue:
                    "batch_prepare")
         self.times = torch.zeros(n + 1, dtype=torch.int64, device=device)
         self.ctas_per_sm = ctas_per_sm
+        self.ensembles = ensembles
+
+    def kernel_launches(self) -> int:
+        """Kernels one launch() enqueues: the persistent kernel, or per ensemble its
+        single-ensemble kernels (64-frame chunks plus a tail launch; XDoppler's
+        magnitude pass; DMAS one) and a completion stamp, plus the start stamp."""
+        if self.ctas_per_sm:
+            return 1
+        total = 1
+        for e in self.ensembles:
+            nt = e.shape[3]
+            das = 1 if e.method == "dmas" else (nt >= 64) + (nt % 64 > 0) + (e.method == "xdoppler")
+            total += das + 1
+        return total
 
     def launch(self, stream) -> None:
         _lib.check(self.lib.rcabeam_batch_run_device(len(self.indices), self.list, self.table.data_ptr() + self.base,
@@ -255,7 +271,10 @@ def autotune(ensembles, *, sample_tiles: int = 148 * 2, repeats: int = 2, cache:
             if not reps:
                 budgets[method] = 1
                 continue
-            results = {k: timed(BatchQueue(reps, ctas_per_sm=k, voxel_limit=64 * sample_tiles)) for k in (1, 2, 3)}
+            # Persistent kernel at 2 or 3 CTAs per SM, or per-ensemble grids (0): which one wins
+            # depends on the ensembles' size, so the sample is eight times the frame-chunk one.
+            results = {k: timed(BatchQueue(reps, ctas_per_sm=k, voxel_limit=8 * 64 * sample_tiles))
+                       for k in (0, 2, 3)}
             budgets[method] = min(results, key=results.get)
         cache["ctas_per_sm"] = budgets
     return {**{str(k): v for k, v in cache.items() if k != "ctas_per_sm"}, "ctas_per_sm": cache["ctas_per_sm"]}

@@ -141,27 +141,14 @@ __device__ __forceinline__ bool staged_dmas(const Queue& q, const das::Args& arg
   return das::consume_dmas_item<kDmasLpv>(args, vox, active, ring, frame0, warp, k);
 }
 
-// Per-ensemble arguments of a short queue, passed in the kernel's parameter
-// space: the DMAS producer's float64 delay chain reads the geometry constants
-// at every step, and from the parameter space they are constant-bank loads the
-// compiler may hoist or repeat at will, where a copy from the global table
-// competes for the 72-register budget (measured: 41 % more instructions for a
-// DMAS ensemble through the table than through the single-ensemble kernel).
-constexpr int kParamEnsembles = 48;  // 48 x 160 B of kernel parameters
-struct ParamArgs {
-  das::Args args[kParamEnsembles];
-};
-
 // Slot width of a queue of kind KIND: 32-frame slots for DMAS alone, else 64.
 template <int KIND>
 __host__ __device__ constexpr int smem_lpv() { return KIND == 3 ? kDmasLpv : 32; }
 
 // MINB resident CTAs per SM (register budget 65536 / (288 MINB)); the
 // autotuner picks the variant.  KIND and TMA as for staged().
-// The DMAS kernel (KIND 3) takes every ensemble's arguments from pa (queues of
-// at most kParamEnsembles); the others read the table.
 template <int MINB, int KIND, int TMA>
-__global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q, const __grid_constant__ ParamArgs pa) {
+__global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q) {
   using Smem = batch::Smem<smem_lpv<KIND>()>;
   extern __shared__ __align__(1024) unsigned char smem[];
   const das::Ring ring{smem + Smem::kData, 0, reinterpret_cast<das::StageTap*>(smem + Smem::kTaps),
@@ -228,12 +215,9 @@ __global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q, const 
         }
       }
     };
-    if constexpr (KIND == 3) {
-      item_body(pa.args[ei]);
-    } else {
-      // The other kernels take a private copy: the table in global memory
-      // could alias the item's stores, so its fields would be reloaded inside
-      // the hot loops.  (From the parameter space the OPW kernel spills.)
+    {
+      // A private copy: the table in global memory could alias the item's
+      // stores, so its fields would be reloaded inside the hot loops.
       const das::Args local = e.args;
       item_body(local);
     }
@@ -262,6 +246,13 @@ __global__ void __launch_bounds__(das::kThreads, MINB) run(const Queue q, const 
     }
   }
   if (warp == das::kConsumerWarps) das::drain_ring(ring, k, q.err);
+}
+
+// Per-ensemble grid mode of the queue: a global-timer stamp after each
+// ensemble's launches (start = 1: the queue's start, kept as a minimum).
+__global__ void stamp(unsigned long long* t, int start) {
+  if (start) atomicMin(t, static_cast<unsigned long long>(global_ns()));
+  else *t = global_ns();
 }
 
 }  // namespace batch

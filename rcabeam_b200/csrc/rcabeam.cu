@@ -190,31 +190,32 @@ static unsigned pow2_at_least(unsigned x) {
 }
 
 template <int LPV, bool HALF, int MODE, bool TMA>
-static rcabeam_status launch_staged(const CUtensorMap& mr, const CUtensorMap& mq, const das::Args& a, dim3 grid) {
+static rcabeam_status launch_staged(const CUtensorMap& mr, const CUtensorMap& mq, const das::Args& a, dim3 grid,
+                                    cudaStream_t stream) {
   using S = das::Shape<LPV, HALF>;
   auto kern = das::opw_staged<LPV, HALF, MODE, TMA>;
   size_t smem = S::bytes(a.na);
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
     return RCABEAM_ERROR_CUDA;
-  kern<<<grid, das::kThreads, smem>>>(mr, mq, a);
+  kern<<<grid, das::kThreads, smem, stream>>>(mr, mq, a);
   return launch_status();
 }
 
 template <bool HALF, int MODE, bool TMA>
 static rcabeam_status launch_lpv(int lpv, const CUtensorMap& mr, const CUtensorMap& mq, const das::Args& a,
-                                 dim3 grid) {
+                                 dim3 grid, cudaStream_t stream) {
   switch (lpv) {
-    case 32: return launch_staged<32, HALF, MODE, TMA>(mr, mq, a, grid);
-    case 16: return launch_staged<16, HALF, MODE, TMA>(mr, mq, a, grid);
-    case 8: return launch_staged<8, HALF, MODE, TMA>(mr, mq, a, grid);
-    case 4: return launch_staged<4, HALF, MODE, TMA>(mr, mq, a, grid);
-    default: return launch_staged<2, HALF, MODE, TMA>(mr, mq, a, grid);
+    case 32: return launch_staged<32, HALF, MODE, TMA>(mr, mq, a, grid, stream);
+    case 16: return launch_staged<16, HALF, MODE, TMA>(mr, mq, a, grid, stream);
+    case 8: return launch_staged<8, HALF, MODE, TMA>(mr, mq, a, grid, stream);
+    case 4: return launch_staged<4, HALF, MODE, TMA>(mr, mq, a, grid, stream);
+    default: return launch_staged<2, HALF, MODE, TMA>(mr, mq, a, grid, stream);
   }
 }
 
 template <bool HALF, int MODE>
-static rcabeam_status run_staged(das::Args a, size_t ntiles) {
+static rcabeam_status run_staged(das::Args a, size_t ntiles, cudaStream_t stream = 0) {
   const int elem = HALF ? 4 : 8;
   const size_t nt = size_t(a.nt);
   const bool aligned = (nt * elem) % 16 == 0 && reinterpret_cast<uintptr_t>(a.rc) % 16 == 0 &&
@@ -239,15 +240,15 @@ static rcabeam_status run_staged(das::Args a, size_t ntiles) {
     das::Args b = a;
     b.frame_base = launches[i].base;
     dim3 grid(unsigned(ntiles), unsigned(launches[i].chunks));
-    rcabeam_status st = tma ? launch_lpv<HALF, MODE, true>(launches[i].lpv, mr, mq, b, grid)
-                            : launch_lpv<HALF, MODE, false>(launches[i].lpv, mr, mq, b, grid);
+    rcabeam_status st = tma ? launch_lpv<HALF, MODE, true>(launches[i].lpv, mr, mq, b, grid, stream)
+                            : launch_lpv<HALF, MODE, false>(launches[i].lpv, mr, mq, b, grid, stream);
     if (st != RCABEAM_SUCCESS) return st;
   }
   return RCABEAM_SUCCESS;
 }
 
 // DMAS-CCF-ACF on the staged pipeline: 32-frame chunks, both passes per CTA.
-static rcabeam_status run_dmas_staged(das::Args a, size_t ntiles) {
+static rcabeam_status run_dmas_staged(das::Args a, size_t ntiles, cudaStream_t stream = 0) {
   constexpr int kLpv = 16;
   using S = das::Shape<kLpv, false>;
   const size_t nt = size_t(a.nt);
@@ -262,7 +263,7 @@ static rcabeam_status run_dmas_staged(das::Args a, size_t ntiles) {
   auto kern = tma ? das::dmas_staged<kLpv, true> : das::dmas_staged<kLpv, false>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
     return RCABEAM_ERROR_CUDA;
-  kern<<<grid, das::kThreads, smem>>>(mr, mq, a);
+  kern<<<grid, das::kThreads, smem, stream>>>(mr, mq, a);
   return launch_status();
 }
 
@@ -603,12 +604,10 @@ static bool project_reg(const void* iq, void* out, double* power, size_t rows, s
 template <typename IN>
 static void project_dispatch(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
                              size_t k, int mode, unsigned* flags) {
-  const char* form = std::getenv("RCABEAM_PROJECT");
-  const bool reg_off = form && (std::string(form) == "one" || std::string(form) == "async");
   if constexpr (sizeof(IN) == 8) {
-    if (!reg_off && project_reg(iq, out, power, rows, nt, vec, k, mode, flags)) return;
+    if (project_reg(iq, out, power, rows, nt, vec, k, mode, flags)) return;
   }
-  if (k <= size_t(clutter::kProjSmall) && !(form && std::string(form) == "one")) {
+  if (k <= size_t(clutter::kProjSmall)) {
     if (nt <= 256 && launch_async<IN, 8>(iq, out, power, rows, nt, vec, k, mode, flags)) return;
     if (nt > 256 && launch_async<IN, 16>(iq, out, power, rows, nt, vec, k, mode, flags)) return;
   }
@@ -1408,7 +1407,7 @@ rcabeam_status rcabeam_batch_run_device(size_t n, const rcabeam_batch_ensemble* 
                                         void* stream) {
   BatchLayout L;
   long long total = 0;
-  if (!table || !times || ctas_per_sm < 1 || ctas_per_sm > 3 || !batch_plan(n, list, nullptr, &L, &total) ||
+  if (!table || !times || ctas_per_sm < 0 || ctas_per_sm > 3 || !batch_plan(n, list, nullptr, &L, &total) ||
       table_bytes < L.total)
     return RCABEAM_ERROR_ARGUMENT;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1422,37 +1421,53 @@ rcabeam_status rcabeam_batch_run_device(size_t n, const rcabeam_batch_ensemble* 
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  std::vector<batch::Ensemble> ens;
+  batch_plan(n, list, &ens, &L, &total);
+  if (ctas_per_sm == 0) {
+    // Grid mode: each ensemble through the single-ensemble kernels on the
+    // stream (for ensembles that fill the GPU alone, where those kernels run
+    // faster than the persistent loop), a completion stamp after each.
+    batch::stamp<<<1, 1, 0, st>>>(times, 1);
+    for (size_t i = 0; i < n; ++i) {
+      const das::Args& a = ens[i].args;
+      const size_t ntiles = (size_t(a.nv) + das::kTileVoxels - 1) / das::kTileVoxels;
+      rcabeam_status r = RCABEAM_SUCCESS;
+      if (list[i].method == 3) {
+        r = run_dmas_staged(a, ntiles, st);
+      } else if (list[i].method == 1) {
+        r = run_staged<false, das::kXdoppler>(a, ntiles, st);
+        if (r == RCABEAM_SUCCESS) das::finish_magnitude<<<unsigned((a.nv + 255) / 256), 256, 0, st>>>(a.pd, a.nv);
+      } else {
+        r = run_staged<false, das::kOpw>(a, ntiles, st);
+      }
+      if (r != RCABEAM_SUCCESS) return r;
+      batch::stamp<<<1, 1, 0, st>>>(times + 1 + i, 0);
+    }
+    return cudaGetLastError() == cudaSuccess ? RCABEAM_SUCCESS : RCABEAM_ERROR_CUDA;
+  }
   // A queue of one method whose ensembles all stage the same way (TMA or plain
   // loads) at two or three CTAs per SM runs the kernel compiled for that
   // method and staging alone; anything else runs the general kernel.
-  std::vector<batch::Ensemble> ens;
-  batch_plan(n, list, &ens, &L, &total);
   int kind = list[0].method, tma = ens[0].tma;
   for (size_t i = 1; i < n; ++i) {
     if (list[i].method != kind) kind = -1;
     if (ens[i].tma != tma) tma = -1;
   }
-  using Kernel = void (*)(const batch::Queue, const batch::ParamArgs);
+  using Kernel = void (*)(const batch::Queue);
   static const Kernel general[3] = {batch::run<1, -1, -1>, batch::run<2, -1, -1>, batch::run<3, -1, -1>};
   static const Kernel special[3][2][2] = {  // [kind][tma][ctas_per_sm - 2]
       {{batch::run<2, 0, 0>, batch::run<3, 0, 0>}, {batch::run<2, 0, 1>, batch::run<3, 0, 1>}},
       {{batch::run<2, 1, 0>, batch::run<3, 1, 0>}, {batch::run<2, 1, 1>, batch::run<3, 1, 1>}},
       {{batch::run<2, 3, 0>, batch::run<3, 3, 0>}, {batch::run<2, 3, 1>, batch::run<3, 3, 1>}},
   };
-  const bool specific = kind >= 0 && tma >= 0 && ctas_per_sm >= 2 && (kind != 3 || n <= size_t(batch::kParamEnsembles));
+  const bool specific = kind >= 0 && tma >= 0 && ctas_per_sm >= 2;
   const Kernel kern = specific ? special[kind == 3 ? 2 : kind][tma][ctas_per_sm - 2] : general[ctas_per_sm - 1];
   const size_t smem = specific && kind == 3 ? batch::Smem<batch::smem_lpv<3>()>::kBytes : batch::Smem<32>::kBytes;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
     return RCABEAM_ERROR_CUDA;
   const long long want = (long long)sms * ctas_per_sm;
   const unsigned grid = unsigned(total < want ? total : want);
-  static batch::ParamArgs pa;  // host staging of the launch's parameters (copied at launch)
-  static std::mutex pa_lock;
-  std::lock_guard<std::mutex> guard(pa_lock);
-  pa = batch::ParamArgs{};
-  if (specific && kind == 3)
-    for (size_t i = 0; i < n; ++i) pa.args[i] = ens[i].args;
-  kern<<<grid, das::kThreads, smem, st>>>(batch_queue(table, n, L, total, times), pa);
+  kern<<<grid, das::kThreads, smem, st>>>(batch_queue(table, n, L, total, times));
   return cudaGetLastError() == cudaSuccess ? RCABEAM_SUCCESS : RCABEAM_ERROR_CUDA;
 }
 
