@@ -442,7 +442,8 @@ def run_batching(args) -> dict:
         "power_rel_l2_batch_vs_sequential_max": worst,
         "autotune": {**choice, "seconds": round(tune_s, 2)},
         "launches": "per method either one persistent kernel (own register budget) or the single-ensemble "
-                    "kernels launched per ensemble, as the autotuner measured faster; forked streams, one CUDA graph",
+                    "kernels launched per ensemble, as the autotuner measured faster; methods one after another "
+                    "on one stream, one CUDA graph",
         "mode_by_method": {p.ensembles[0].method: ("per-ensemble grids" if p.ctas_per_sm == 0
                                                    else f"persistent, {p.ctas_per_sm} CTAs/SM")
                            for p in queue.parts},

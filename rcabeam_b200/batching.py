@@ -1,21 +1,20 @@
-"""Batching form: a queue of uneven ensembles through persistent kernels under one CUDA graph.
+"""Batching form: a queue of uneven ensembles under one CUDA graph.
 
 ``BatchQueue`` holds device-resident ensembles (packed RC/CR channels, grid,
-geometry, method).  The queue is split by method into sub-queues, and each
-sub-queue is reconstructed by one launch of the persistent batch kernel
-(``rcabeam_batch_run_device``) with its own register budget (resident CTAs
-per SM): OPW and XDoppler tiles run the TMA-staged pipeline at one budget,
-DMAS-CCF-ACF's two-pass pipeline at another.  One register budget for all three
-methods made the single persistent launch slower than sequential launches
-(the OPW / XDoppler consumers spill at DMAS's budget, DMAS loses latency
-hiding at theirs).  The sub-queue launches run on forked streams and are
-captured together into one CUDA graph; within a launch, persistent CTAs take
-items from a global counter in queue order, so small and large ensembles
-share the GPU without launch gaps or per-ensemble tails.  ``autotune`` picks,
-per ensemble shape class, the frame chunk of the staged pipeline and, per
-method, the resident CTAs per SM, by timing candidates on bounded samples of
-the ensembles.  Per-ensemble completion times come from the kernels (global
-timer), so latencies are measured on the device.
+geometry, traversal order, method).  The queue is split by method into
+sub-queues; each runs either as one launch of the persistent batch kernel
+(``rcabeam_batch_run_device`` with 1-3 CTAs per SM: persistent CTAs take
+(tile, frame chunk) items from a global counter in queue order, so small and
+large ensembles share the GPU without launch gaps or per-ensemble tails, with
+a kernel compiled for that method alone) or as per-ensemble launches of the
+single-ensemble kernels (``ctas_per_sm`` 0), whichever ``autotune`` measures
+faster for that method on bounded samples of its ensembles (it also picks the
+staged pipeline's frame chunk per shape class).  Ensembles that fill the GPU
+alone run the single-ensemble kernels faster than the persistent loop for
+OPW and DMAS-CCF-ACF; XDoppler's persistent kernel is the faster one.  The
+sub-queues run one after another on one stream (run concurrently, their
+sample windows compete for L2) and the whole queue is captured into one CUDA
+graph.  Per-ensemble completion times come from the device's global timer.
 
 Methods: "opw" (power of the coherent sum), "xdoppler" (|mean r conj(q)|) and
 "dmas" (DMAS-CCF-ACF), as in ``ensemble_pd_from_channels`` (reference
@@ -172,24 +171,22 @@ class BatchQueue:
         self.ensembles = list(ensembles)
         device = self.ensembles[0].rc.device
         budget = ctas_per_sm if isinstance(ctas_per_sm, dict) else {m: int(ctas_per_sm) for m in METHODS}
-        # Longest-running methods first: later launches fill the SMs that earlier ones leave idle.
+        # One sub-queue after another on one stream: run concurrently, the methods'
+        # sample windows compete for L2 (measured 129.7 s against 109.6 s for the
+        # sequential launches on the 48-ensemble queue, with the same kernels).
         self.parts = []
         for method in ("dmas", "opw", "xdoppler"):
             idx = [i for i, e in enumerate(self.ensembles) if e.method == method]
             if idx:
                 self.parts.append(_SubQueue(self.lib, idx, [self.ensembles[i] for i in idx], int(budget[method]),
                                             voxel_limit, device))
-        self.streams = [torch.cuda.Stream(device) for _ in self.parts]
         self.graph = None
 
     def launch(self, stream: torch.cuda.Stream | None = None) -> None:
-        """Fork the sub-queue launches onto their streams from ``stream`` and join them back."""
+        """Enqueue the sub-queues one after another on ``stream`` (default: the current stream)."""
         main = torch.cuda.current_stream() if stream is None else stream
-        for part, side in zip(self.parts, self.streams):
-            side.wait_stream(main)
-            part.launch(side)
-        for side in self.streams:
-            main.wait_stream(side)
+        for part in self.parts:
+            part.launch(main)
 
     def capture(self) -> None:
         """Record the launches into one CUDA graph (the first run warms up outside the capture)."""
