@@ -503,32 +503,49 @@ __global__ void __launch_bounds__(kAsyncThreads, 2)
 // float64 arithmetic only (the shared-memory form reads 2 K F double2 per
 // lane and row back, about twice the shared-memory cycles its float64 work
 // takes).  Same sums in the same order as project_rows_async.
+// H = 2 extends it to 256 < nt <= 512: a row per pair of warps, warp h of the
+// pair holding frames 32 F h + l + 32 f; the pair adds its two partial
+// coordinates (and partial powers) through shared memory behind a 64-thread
+// named barrier, half 0 first in both warps.
 constexpr int kRegThreads = 128;
 constexpr int kRegWarps = kRegThreads / 32;
 
-template <int F, int K>
+__host__ __device__ inline size_t reg_smem_bytes(size_t nt) {
+  return size_t(kRegWarps) * kAsyncDepth * nt * sizeof(float2) + size_t(kRegWarps) * 4 * sizeof(double2);
+}
+
+template <int F, int K, int H>
 __global__ void __launch_bounds__(kRegThreads, 3)
     project_rows_reg(const float2* __restrict__ x, float2* __restrict__ out, double* __restrict__ power,
                      size_t rows, int nt, const double2* __restrict__ vec, int mode, double inv_nt,
                      unsigned* __restrict__ flags) {
+  static_assert(H == 1 || H == 2, "one or two warps per row");
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pair = warp / H, half = warp % H;
   float2* ring = reinterpret_cast<float2*>(smem) + size_t(warp) * kAsyncDepth * nt;
+  // Exchange slots of a pair: [half][K] coordinates, then [half] partial power.
+  double2* xch = reinterpret_cast<double2*>(smem + size_t(kRegWarps) * kAsyncDepth * nt * sizeof(float2)) +
+                 size_t(pair) * 2 * 4;
+  const int t0 = 32 * F * half;  // first frame of this warp's half
   double2 v[K][F];
 #pragma unroll
   for (int c = 0; c < K; ++c)
 #pragma unroll
     for (int f = 0; f < F; ++f) {
-      const int t = lane + 32 * f;
+      const int t = t0 + lane + 32 * f;
       v[c][f] = t < nt ? vec[c * nt + t] : make_double2(0.0, 0.0);
     }
-  const size_t stride = size_t(gridDim.x) * kRegWarps;
-  size_t row = size_t(blockIdx.x) * kRegWarps + warp;
+  auto pair_sync = [&]() {
+    if constexpr (H == 2) asm volatile("bar.sync %0, 64;" ::"r"(1 + pair) : "memory");
+  };
+  const size_t stride = size_t(gridDim.x) * (kRegWarps / H);
+  size_t row = size_t(blockIdx.x) * (kRegWarps / H) + pair;
   auto issue = [&](size_t r, int slot) {
     if (r < rows) {
 #pragma unroll
       for (int f = 0; f < F; ++f) {
-        const int t = lane + 32 * f;
+        const int t = t0 + lane + 32 * f;
         if (t < nt) async_copy(ring + slot * nt + t, x + r * nt + t);
       }
     }
@@ -545,7 +562,7 @@ __global__ void __launch_bounds__(kRegThreads, 3)
     double2 xv[F];
 #pragma unroll
     for (int f = 0; f < F; ++f) {
-      const int t = lane + 32 * f;
+      const int t = t0 + lane + 32 * f;
       if (t < nt) {
         const float2 a = cur[t];
         xv[f] = make_double2(double(a.x), double(a.y));
@@ -555,7 +572,6 @@ __global__ void __launch_bounds__(kRegThreads, 3)
       }
     }
     double2 y[K];
-    double retained = 0.0;
 #pragma unroll
     for (int c = 0; c < K; ++c) {
       double yr = 0.0, yi = 0.0;
@@ -570,13 +586,24 @@ __global__ void __launch_bounds__(kRegThreads, 3)
         yi += __shfl_xor_sync(0xffffffffu, yi, off);
       }
       y[c] = make_double2(yr, yi);
-      retained += yr * yr + yi * yi;
     }
+    if constexpr (H == 2) {  // the pair's two halves, half 0 first
+      if (lane == 0)
+#pragma unroll
+        for (int c = 0; c < K; ++c) xch[half * 4 + c] = y[c];
+      pair_sync();
+#pragma unroll
+      for (int c = 0; c < K; ++c)
+        y[c] = make_double2(xch[c].x + xch[4 + c].x, xch[c].y + xch[4 + c].y);
+    }
+    double retained = 0.0;
+#pragma unroll
+    for (int c = 0; c < K; ++c) retained += y[c].x * y[c].x + y[c].y * y[c].y;
     double pw = 0.0;
     if (mode & 3) {
 #pragma unroll
       for (int f = 0; f < F; ++f) {
-        const int t = lane + 32 * f;
+        const int t = t0 + lane + 32 * f;
         if (t < nt) {
           double2 proj = make_double2(0.0, 0.0);
 #pragma unroll
@@ -594,14 +621,20 @@ __global__ void __launch_bounds__(kRegThreads, 3)
       if (subtract) {
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) pw += __shfl_xor_sync(0xffffffffu, pw, off);
+        if constexpr (H == 2) {  // slot 3 of each half holds its partial power
+          if (lane == 0) xch[half * 4 + 3].x = pw;
+          pair_sync();
+          pw = xch[3].x + xch[4 + 3].x;
+        }
       } else {
         pw = retained;
       }
-      if (lane == 0) {
+      if (lane == 0 && half == 0) {
         power[row] = pw * inv_nt;
         bad_out |= !isfinite(pw);
       }
     }
+    pair_sync();  // the exchange slots are read before the next row writes them
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
   if (flags) {

@@ -570,34 +570,37 @@ static bool launch_async(const void* iq, void* out, double* power, size_t rows, 
   return true;
 }
 
-template <int F, int K>
+template <int F, int K, int H>
 static void launch_reg(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
                        int mode, unsigned* flags) {
-  auto kern = clutter::project_rows_reg<F, K>;
-  const size_t smem = size_t(clutter::kRegWarps) * clutter::kAsyncDepth * nt * sizeof(float2);
+  auto kern = clutter::project_rows_reg<F, K, H>;
+  const size_t smem = clutter::reg_smem_bytes(nt);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   int dev = 0, sms = 148, per_sm = 3;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, clutter::kRegThreads, smem);
-  const size_t want = (rows + clutter::kRegWarps - 1) / clutter::kRegWarps;
+  const size_t rows_per_block = clutter::kRegWarps / H;
+  const size_t want = (rows + rows_per_block - 1) / rows_per_block;
   const size_t grid = std::min(want, size_t(sms) * size_t(per_sm > 0 ? per_sm : 1));
   kern<<<unsigned(grid), clutter::kRegThreads, smem>>>(static_cast<const float2*>(iq), static_cast<float2*>(out),
                                                         power, rows, int(nt), reinterpret_cast<const double2*>(vec),
                                                         mode, 1.0 / double(nt), flags);
 }
 
-// Complex64, 1-3 vectors, 33-256 frames: the register form.
+// Complex64, 1-3 vectors, 33-512 frames: the register form (a warp pair per
+// row above 256 frames).
 static bool project_reg(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
                         size_t k, int mode, unsigned* flags) {
-  if (k < 1 || k > 3 || nt <= 32 || nt > 256) return false;
+  if (k < 1 || k > 3 || nt <= 32 || nt > 512) return false;
   const int f = int((nt + 31) / 32);
   using Launch = void (*)(const void*, void*, double*, size_t, size_t, const double*, int, unsigned*);
-  static const Launch table[3][3] = {  // [k - 1][F = 4, 7, 8]
-      {launch_reg<4, 1>, launch_reg<7, 1>, launch_reg<8, 1>},
-      {launch_reg<4, 2>, launch_reg<7, 2>, launch_reg<8, 2>},
-      {launch_reg<4, 3>, launch_reg<7, 3>, launch_reg<8, 3>},
+  static const Launch table[3][4] = {  // [k - 1][F = 4, 7, 8 on one warp; 8 on a warp pair]
+      {launch_reg<4, 1, 1>, launch_reg<7, 1, 1>, launch_reg<8, 1, 1>, launch_reg<8, 1, 2>},
+      {launch_reg<4, 2, 1>, launch_reg<7, 2, 1>, launch_reg<8, 2, 1>, launch_reg<8, 2, 2>},
+      {launch_reg<4, 3, 1>, launch_reg<7, 3, 1>, launch_reg<8, 3, 1>, launch_reg<8, 3, 2>},
   };
-  table[k - 1][f <= 4 ? 0 : f <= 7 ? 1 : 2](iq, out, power, rows, nt, vec, mode, flags);
+  table[k - 1][f <= 4 ? 0 : f <= 7 ? 1 : f <= 8 ? 2 : 3](iq, out, power, rows, nt, vec, mode, flags);
   return true;
 }
 
