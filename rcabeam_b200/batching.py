@@ -87,7 +87,7 @@ class Ensemble:
         t = dict(scan=scan, xe=f32(self.geom.x_el), ye=f32(self.geom.y_el), angles=f32(self.angles),
                  starts=f32(np.broadcast_to(np.asarray(self.t_start, np.float32), (na,))),
                  pd=torch.zeros((nv, 2), dtype=torch.float32, device=device), order=None)
-        if order and self.method != "dmas" and nv >= 128:
+        if order and nv >= 128:  # every method's 64-voxel tiles want compact (Morton) voxel sets
             size = ctypes.c_size_t(0)
             _lib.check(_lib.lib().rcabeam_voxel_order_workspace_bytes(nv, ctypes.byref(size)), "voxel_order")
             ws = torch.empty(int(size.value), dtype=torch.uint8, device=device)
