@@ -166,7 +166,8 @@ rcabeam_status rcabeam_pack_ensemble_split_device(const void* source, void* hi, 
  * where the other SMs are, which keeps their sample windows in L2 together but
  * makes the order of the float32 sums depend on timing); the interleaving of
  * the builder warps still varies, so repeated calls agree to about 1e-7 of the
- * IQ instead of being bit-identical.  Coefficients are
+ * IQ instead of being bit-identical; the unaligned walk costs about 10 % more
+ * time (more of its windows miss L2).  Coefficients are
  * split into hi + lo halves; accumulation is float32.  pd, signal and
  * geometry_workspace are as for rcabeam_ensemble_device (method 0).  Requires
  * nt % 4 == 0 and 16-byte aligned planes (RCABEAM_ERROR_ARGUMENT otherwise).

@@ -46,7 +46,8 @@ class FilteredOpw:
     (by default each tile starts where the other SMs are, which keeps their
     windows in L2 together but makes the order of the float32 sums timing
     dependent); the builder warps' interleaving remains timing dependent, so
-    reruns agree to 2e-6 - 1e-5 in filtered power instead of up to 5e-5."""
+    reruns agree to 2e-6 - 1e-5 in filtered power instead of up to 5e-5, at about
+    10 % more DAS time (measured 921 against 834 ms at the full-size workload)."""
 
     def __init__(self, channel_shape, angles, t_start, grid, geom: RCAGeometry, *, rank_start: int = 3,
                  rank_stop: int | None = None, precision: str = "complex128", iq_storage: str = "float32",
