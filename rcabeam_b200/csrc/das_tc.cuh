@@ -15,9 +15,9 @@
 // and lane 2v + 1 holds Q = Im(A) X, and the voxel's IQ is
 // (P_re - Q_im) + j (P_im + Q_re).  Both 64-voxel groups of a tile use the
 // same staged window (two MMAs per product), which halves the window bytes
-// per interpolated sample.  Frames run in passes of 128 (N = 256: four whole
-// 64-column TMA boxes per plane) and a last pass of the remainder rounded up
-// to 8 frames, so no staged column is wasted except in the last box.
+// per interpolated sample.  Frames run in passes of nearly equal length (at
+// most 128 frames, N <= 256, multiples of 8 frames; 200 = 104 + 96), so that
+// every work item costs about the same and the CTAs' walks stay together.
 //
 // Precision: FP16-packed channels are exact FP16 and the coefficients are
 // split into FP16 hi + lo (two products, coefficients scaled by 2^10 so the lo

@@ -279,8 +279,14 @@ static bool tc_eligible(const void* const* planes, int count, size_t nt) {
 // Frame passes of the tensor-core OPW: full passes of 128 frames (N = 256, four
 // whole 64-column boxes per plane) and a last pass with the remainder rounded up
 // to 8 frames, which stages fewer boxes than equal passes would.
+// Frames of every frame pass but the last: passes of nearly equal length
+// (multiples of 8 frames, at most kMaxFrames).  Equal passes keep the CTAs'
+// items equally long, so the herd's channel walks stay aligned (200 frames:
+// 104 + 96 ran the DAS 2.5 % faster than 128 + 72).
 static size_t tc_full_frames(size_t nt) {
-  return nt > size_t(tc::kMaxFrames) ? size_t(tc::kMaxFrames) : (nt + 7) / 8 * 8;
+  if (nt <= size_t(tc::kMaxFrames)) return (nt + 7) / 8 * 8;
+  const size_t passes = (nt + tc::kMaxFrames - 1) / tc::kMaxFrames;
+  return ((nt + passes - 1) / passes + 7) / 8 * 8;
 }
 
 static size_t tc_smem_bytes(bool bf16x3, size_t nt, size_t na, int stages = tc::kStages) {
