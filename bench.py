@@ -53,10 +53,10 @@ T_START = 4e-6
 RANK_START = 3
 # DRAM bytes (read + write) of one full-size bf16x3 tensor-core DAS launch, from
 # an ncu capture of that launch (dram__bytes_read.sum + dram__bytes_write.sum).
-DAS_DRAM_BYTES_PER_LAUNCH = 573_671_879_168 + 42_624_266_752
+DAS_DRAM_BYTES_PER_LAUNCH = 552_474_713_344 + 42_600_415_232
 DAS_DRAM_SOURCE = ("ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum "
                    "--clock-control none -k regex:opw_tc -c 1 on the full-size flow-scene step (a 1-pass metric "
-                   "set): 573.7 GB read + 42.6 GB written in one 820 ms launch; the writes are the 512-step "
+                   "set): 552.5 GB read + 42.6 GB written in one 800.6 ms launch; the writes are the 512-step "
                    "segment flushes into the complex64 IQ, the reads plane windows that missed L2")
 # DAS unit model: FP32-equivalent operations per interpolated sample -- the
 # lerp's two differences, two lerp FFMA and four FFMA of the complex rotate-
