@@ -25,7 +25,9 @@
 // planes; with BF16 hi/lo coefficients each step runs three products
 // (Ahi Xhi + Alo Xhi + Ahi Xlo).  Accumulation is float32 in TMEM.
 //
-// Roles (one CTA per SM, persistent over (tile, frame pass)), with S ring
+// Roles (one CTA per SM, persistent over (tile, frame pass) work items that
+// the builders take from a global counter and tag every staged slot with, so
+// the MMA warp and the epilogue follow them), with S ring
 // stages (the deepest of 6..2 that fits shared memory; 352 threads x 168
 // registers at six stages still fit the register file):
 //   warps 0..S-1  builders, one per ring stage.  A warp owns whole steps:
@@ -89,7 +91,7 @@ enum Meta : int { kStep = 0, kTileEnd = 1, kFinish = 2 };
 constexpr int kSegSteps = 512;
 constexpr int kMaxCtas = 160;
 constexpr size_t kPartialPerCta = size_t(2) * kGroupVox * kMaxFrames;  // float2 per CTA
-enum AccKind : int { kAccPartial = 0, kAccFinal = 1, kAccFinalEmpty = 2 };
+enum AccKind : int { kAccPartial = 0, kAccFinal = 1, kAccFinalEmpty = 2, kAccDone = 3 };
 
 struct Args {
   const void* x_hi[2];  // per aperture (RC, CR): FP16 or BF16 hi planes, packed (c, a, s, 2 nt)
@@ -114,6 +116,7 @@ struct Args {
   int ntiles;
   int walk_fixed;  // 1: every item walks the channel slots from slot 0 (no timing-dependent start)
   int seg_steps;   // MMA steps between accumulator flushes (float32 accumulation length)
+  unsigned* item_counter;  // next work item to take (zeroed before the launch); nullptr: CTA b takes b, b + G, ...
   int* err;
 };
 
@@ -355,6 +358,9 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
   int* item_steps = counter + 1;                         // steps staged for the current item
   volatile int* acc_kind = item_steps + 1;               // AccKind of the pending flush
   int* walk_start = item_steps + 2;                      // first channel slot of the current item
+  int* grab = item_steps + 3;                            // the builders' current item (taken from the counter)
+  volatile int* acc_item = item_steps + 4;               // work item of the pending flush
+  int* meta_item = item_steps + 5;                       // [STAGES]: work item of each staged slot
   double* angle_tab = reinterpret_cast<double*>(ctrl + kCtrlBytes);
   // Transmit delay of (aperture, angle, voxel) = tx_base[aperture, angle] (the
   // tile's first voxel, float64) + tx_off (float: within a compact tile the
@@ -448,7 +454,18 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
       }
       if (lane != 0) mbar_arrive(&full[s]);
     };
-    for (int item = blockIdx.x; item < work_items; item += gridDim.x) {
+    for (int next = blockIdx.x;; next += gridDim.x) {
+      // The next work item: b, b + G, ... for CTA b, or, with p.item_counter,
+      // the next one not yet taken by any CTA (the CTAs then stay within a
+      // window of consecutive items however their items' costs differ).
+      int item = next;
+      if (p.item_counter) {
+        builders_sync();  // every builder has read the previous item's number
+        if (warp == 0 && lane == 0) *grab = int(atomicAdd(p.item_counter, 1u));
+        builders_sync();
+        item = *grab;
+      }
+      if (item >= work_items) break;
       const int tile = item / p.chunks, chunk = item_pass(p, item);
       const int col0 = 2 * chunk * p.frames;
       nbox = pass_boxes(pass_frames(p, chunk));
@@ -562,7 +579,10 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
                 put_rows(a_hi, m, pl, re_hi[j], im_hi[j]);
                 put_rows(a_hi + kAMatBytes, m, pl, re_lo[j], im_lo[j]);
               }
-              if (lane == 0) meta[s] = kStep;
+              if (lane == 0) {
+                meta[s] = kStep;
+                meta_item[s] = item;
+              }
               fence_async_smem();
               mbar_arrive(&full[s]);
               ++steps;
@@ -593,7 +613,10 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
               put_row<BF16X3>(stage + 2 * g * kAMatBytes, stage + (2 * g + 1) * kAMatBytes, m, -1, 0.f, 0.f);
               put_row<BF16X3>(stage + 2 * g * kAMatBytes, stage + (2 * g + 1) * kAMatBytes, m + 1, -1, 0.f, 0.f);
             }
-            if (lane == 0) meta[s] = kStep;
+            if (lane == 0) {
+              meta[s] = kStep;
+              meta_item[s] = item;
+            }
             fence_async_smem();
             stage_window(s, stage, 0, col0, p.ns, 0);
           }
@@ -601,7 +624,10 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
         uint32_t k = 0;
         if (ok) ok = claim(k);
         if (ok) {
-          if (lane == 0) meta[k % STAGES] = kTileEnd;
+          if (lane == 0) {
+            meta[k % STAGES] = kTileEnd;
+            meta_item[k % STAGES] = item;
+          }
           mbar_arrive(&full[k % STAGES]);
         }
       }
@@ -623,15 +649,17 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
   } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------------- MMA --
     if (lane == 0) {
-      // N of the current item's pass; the item advances at every tile-end marker.
-      int mma_item = blockIdx.x;
-      uint32_t idesc = instr_desc(BF16X3, 128, 2 * pass_frames(p, item_pass(p, mma_item)));
+      // The MMA shape (N) follows the pass of the work item each staged slot
+      // is tagged with; every flush hands the epilogue its item.
+      int cur_item = -1;
+      uint32_t idesc = 0;
       uint32_t k = 0, flushes = 0;
       bool need_empty = false;  // a flush is outstanding: the epilogue must drain TMEM first
       bool issued = false;      // MMAs issued since the last flush
       int seg = 0;              // steps in the current segment
-      auto flush = [&](int kind) {
+      auto flush = [&](int kind, int item) {
         *acc_kind = kind;
+        *acc_item = item;
         mma_commit(acc_full);  // arrives once the segment's MMAs have completed
         mbar_arrive(acc_full);
         ++flushes;
@@ -643,19 +671,24 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
         const int s = k % STAGES;
         if (!wait_phase(&full[s], (k / STAGES) & 1, p.err, kErrWaitFull)) break;
         const int m = meta[s];
-        if (m == kFinish) break;
         if (need_empty) {
           if (!mbar_wait(acc_empty, (flushes - 1) & 1, p.err, kErrWaitEmpty)) break;
           need_empty = false;
         }
+        if (m == kFinish) {
+          flush(kAccDone, -1);  // the epilogue has drained every flush: no further item
+          break;
+        }
         tc_fence_after();
         if (m == kTileEnd) {
-          flush(issued ? kAccFinal : kAccFinalEmpty);
+          flush(issued ? kAccFinal : kAccFinalEmpty, meta_item[s]);
           mbar_arrive(&empty[s]);
           ++k;
-          mma_item += gridDim.x;
-          if (mma_item < work_items) idesc = instr_desc(BF16X3, 128, 2 * pass_frames(p, item_pass(p, mma_item)));
           continue;
+        }
+        if (meta_item[s] != cur_item) {
+          cur_item = meta_item[s];
+          idesc = instr_desc(BF16X3, 128, 2 * pass_frames(p, item_pass(p, cur_item)));
         }
         const uint32_t st = smem_u32(stages + size_t(s) * stage_bytes);
         const uint32_t b_hi = st + 4 * kAMatBytes;
@@ -674,7 +707,7 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
         issued = true;
         mma_commit(&empty[s]);  // frees the stage once these MMAs have read it
         ++k;
-        if (++seg == p.seg_steps) flush(kAccPartial);
+        if (++seg == p.seg_steps) flush(kAccPartial, cur_item);
       }
       // Every issued MMA has completed before the warp leaves (TMEM is freed after).
       mma_commit(drain);
@@ -688,17 +721,18 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
     const bool is_p = (m & 1) == 0;
     float2* part = p.partial + size_t(blockIdx.x) * kPartialPerCta;
     uint32_t flushes = 0;
-    bool fail = false;
-    for (int item = blockIdx.x; item < work_items && !fail; item += gridDim.x) {
-      const int tile = item / p.chunks, chunk = item_pass(p, item);
-      const int f0 = chunk * p.frames;
-      const int frames = pass_frames(p, chunk);
-      for (int nflush = 0;; ++nflush) {
-        if (!__all_sync(0xffffffffu, mbar_wait(acc_full, flushes & 1, p.err, kErrWaitFull))) {
-          fail = true;
-          break;
-        }
+    int prev_item = -1, nflush = 0;  // nflush: earlier flushes of the same item
+    {
+      for (;;) {
+        if (!__all_sync(0xffffffffu, mbar_wait(acc_full, flushes & 1, p.err, kErrWaitFull))) break;
         const int kind = *acc_kind;
+        if (kind == kAccDone) break;
+        const int item = *acc_item;
+        nflush = item == prev_item ? nflush + 1 : 0;
+        prev_item = item;
+        const int tile = item / p.chunks, chunk = item_pass(p, item);
+        const int f0 = chunk * p.frames;
+        const int frames = pass_frames(p, chunk);
         tc_fence_after();
         const bool last = kind != kAccPartial;
         for (int g = 0; g < 2; ++g) {
@@ -755,7 +789,6 @@ __global__ void __launch_bounds__(threads_for(STAGES), 1)
         __syncwarp();
         if (lane == 0) mbar_arrive(acc_empty);
         ++flushes;
-        if (last) break;
       }
     }
   }

@@ -302,6 +302,9 @@ static size_t tc_smem_bytes(bool bf16x3, size_t nt, size_t na, int stages = tc::
 // Segment sums of the tensor-core DAS (one slice per resident CTA; launches
 // are serialized on the default stream, so one buffer per device suffices).
 static __device__ float2 g_tc_partials[tc::kMaxCtas * tc::kPartialPerCta];
+// Work-item counter of the tensor-core DAS (one launch at a time per device,
+// like the segment scratch above).
+static __device__ unsigned g_tc_items;
 
 // Global channel-slot count of the tensor-core DAS (its phase aligns the CTAs'
 // slab walks; any starting value works, so it is never reset).
@@ -384,6 +387,13 @@ static rcabeam_status run_tc(tc::Args a) {
   if (!a.partial || !a.slot_clock) return RCABEAM_ERROR_CUDA;
   const int items = a.ntiles * a.chunks;
   const unsigned grid = unsigned(std::min(std::min(items, sms), tc::kMaxCtas));
+  // CTAs take work items from a counter (zeroed here, on the launch's stream):
+  // DAS 826 -> 803 ms at the full-size workload against the static b, b + G, ...
+  void* counter = nullptr;
+  if (cudaGetSymbolAddress(&counter, g_tc_items) != cudaSuccess ||
+      cudaMemsetAsync(counter, 0, sizeof(unsigned), 0) != cudaSuccess)
+    return RCABEAM_ERROR_CUDA;
+  a.item_counter = static_cast<unsigned*>(counter);
   kern<<<grid, tc::threads_for(stages), smem>>>(mh[0], mh[1], ml[0], ml[1], a);
   return launch_status();
 }
