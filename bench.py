@@ -53,10 +53,10 @@ T_START = 4e-6
 RANK_START = 3
 # DRAM bytes (read + write) of one full-size bf16x3 tensor-core DAS launch, from
 # an ncu capture of that launch (dram__bytes_read.sum + dram__bytes_write.sum).
-DAS_DRAM_BYTES_PER_LAUNCH = 552_474_713_344 + 42_600_415_232
+DAS_DRAM_BYTES_PER_LAUNCH = 277_508_977_152 + 41_535_534_848
 DAS_DRAM_SOURCE = ("ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum "
                    "--clock-control none -k regex:opw_tc -c 1 on the full-size flow-scene step (a 1-pass metric "
-                   "set): 552.5 GB read + 42.6 GB written in one 800.6 ms launch; the writes are the 512-step "
+                   "set): 277.5 GB read + 41.5 GB written in one 797.6 ms launch; the writes are the 512-step "
                    "segment flushes into the complex64 IQ, the reads plane windows that missed L2")
 # DAS unit model: FP32-equivalent operations per interpolated sample -- the
 # lerp's two differences, two lerp FFMA and four FFMA of the complex rotate-
