@@ -350,7 +350,10 @@ def run_b200(args, rank: int, world: int) -> dict | None:
             "issued_mma_tflops": round(mma_flops / das_s / 1e12, 1),
             "issued_mma_frac_of_bf16": round(mma_flops / das_s / 1e12 / tensor_peak, 4),
             "bf16_peak_tflops": tensor_peak, "peak_source": peak_source,
-            "traffic": DAS_DRAM_BYTES_PER_LAUNCH, "traffic_source": DAS_DRAM_SOURCE,
+            # The capture is of the full-size launch: a reduced profiling workload has none.
+            "traffic": None if "REDUCED" in CONFIG["workload"] else DAS_DRAM_BYTES_PER_LAUNCH,
+            "traffic_source": ("not captured for a reduced workload" if "REDUCED" in CONFIG["workload"]
+                               else DAS_DRAM_SOURCE),
             "compulsory_hbm_bytes": das_bytes,
             "note": f"compulsory HBM bytes {das_bytes / 1e9:.2f} GB per launch -> {das_bytes / das_s / 1e9:.1f} GB/s: "
                     "the DAS cannot be HBM-bound on algorithmic bytes"},
