@@ -502,13 +502,52 @@ __global__ void __launch_bounds__(kAsyncThreads, 2)
 // in registers for the whole launch, so a row costs its samples' read and
 // float64 arithmetic only (the shared-memory form reads 2 K F double2 per
 // lane and row back, about twice the shared-memory cycles its float64 work
-// takes).  Same sums in the same order as project_rows_async.
+// takes).  The coordinates' warp sums run as one reduce-scatter
+// (warp_sum_coordinates), so their float64 sum order differs from
+// project_rows_async's butterflies (last-bit differences).
 // H = 2 extends it to 256 < nt <= 512: a row per pair of warps, warp h of the
 // pair holding frames 32 F h + l + 32 f; the pair adds its two partial
 // coordinates (and partial powers) through shared memory behind a 64-thread
 // named barrier, half 0 first in both warps.
 constexpr int kRegThreads = 128;
 constexpr int kRegWarps = kRegThreads / 32;
+
+// Warp sums of the 2K partial coordinate components (re, im of each vector),
+// returned to every lane: a reduce-scatter over the padded power of two P of
+// components (at each of the first log2 P xor levels a lane keeps the half its
+// lane bit selects and receives the partner's partial of that half; P - 1
+// shuffles), butterflies over the remaining levels for the one component a
+// lane then holds, and a gather from the lanes 4i that hold component i.  For
+// K = 3 that is 15 float64 shuffles per row instead of 30 for six butterfly
+// sums.
+template <int K>
+__device__ __forceinline__ void warp_sum_coordinates(const double (&part)[2 * K], int lane, double2 (&y)[K]) {
+  constexpr int V = 2 * K;
+  constexpr int P = V <= 2 ? 2 : V <= 4 ? 4 : 8;
+  constexpr int L = P == 2 ? 1 : P == 4 ? 2 : 3;  // reduce-scatter levels
+  double w[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i) w[i] = i < V ? part[i] : 0.0;
+#pragma unroll
+  for (int l = 0; l < L; ++l) {
+    const int off = 16 >> l, half = (P >> l) / 2;
+    const bool upper = lane & off;
+#pragma unroll
+    for (int i = 0; i < half; ++i) {
+      const double give = upper ? w[i] : w[half + i];
+      const double keep = upper ? w[half + i] : w[i];
+      w[i] = keep + __shfl_xor_sync(0xffffffffu, give, off);
+    }
+  }
+  double mine = w[0];  // component ((lane >> (5 - L)) of the padded P)
+#pragma unroll
+  for (int off = 16 >> L; off > 0; off >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, off);
+  constexpr int kSpan = 32 / P;  // lanes per component after the reduce-scatter
+#pragma unroll
+  for (int c = 0; c < K; ++c)
+    y[c] = make_double2(__shfl_sync(0xffffffffu, mine, (2 * c) * kSpan),
+                        __shfl_sync(0xffffffffu, mine, (2 * c + 1) * kSpan));
+}
 
 __host__ __device__ inline size_t reg_smem_bytes(size_t nt) {
   return size_t(kRegWarps) * kAsyncDepth * nt * sizeof(float2) + size_t(kRegWarps) * 4 * sizeof(double2);
@@ -571,7 +610,7 @@ __global__ void __launch_bounds__(kRegThreads, 3)
         xv[f] = make_double2(0.0, 0.0);
       }
     }
-    double2 y[K];
+    double part[2 * K];
 #pragma unroll
     for (int c = 0; c < K; ++c) {
       double yr = 0.0, yi = 0.0;
@@ -580,13 +619,11 @@ __global__ void __launch_bounds__(kRegThreads, 3)
         yr = fma(xv[f].x, v[c][f].x, fma(-xv[f].y, v[c][f].y, yr));
         yi = fma(xv[f].x, v[c][f].y, fma(xv[f].y, v[c][f].x, yi));
       }
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        yr += __shfl_xor_sync(0xffffffffu, yr, off);
-        yi += __shfl_xor_sync(0xffffffffu, yi, off);
-      }
-      y[c] = make_double2(yr, yi);
+      part[2 * c] = yr;
+      part[2 * c + 1] = yi;
     }
+    double2 y[K];
+    warp_sum_coordinates<K>(part, lane, y);
     if constexpr (H == 2) {  // the pair's two halves, half 0 first
       if (lane == 0)
 #pragma unroll

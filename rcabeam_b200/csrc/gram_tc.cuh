@@ -9,8 +9,8 @@
 // 64-frame tile b of G, the tiling the float64 Gram and its finish kernel use).
 //
 // Work: the upper blocks (b <= c) are packed into units of up to four output
-// blocks whose operands fit six staged 128-column blocks (rows b and nb-1-b are
-// paired so most units are full); every unit runs on `slices` CTAs, each over
+// blocks that stage at most three 128-column blocks (plan_units: triangles
+// {a, b, c} first); every unit runs on `slices` CTAs, each over
 // one contiguous range of rows, so the CTAs of one slice read the same rows at
 // the same time (one HBM read, the rest from L2).  TMEM holds the unit's four
 // 128 x 128 float32 accumulators (512 columns); every kFlushRows rows (and at
@@ -32,9 +32,10 @@
 //   warp 1       TMEM allocator; lane 0 issues tcgen05.mma and commits;
 //   warps 2-7    converters: TF32 rounds the staged floats in place (the
 //                layouts coincide), so the staging ring is the operand ring
-//                and is 4 stages deep; 3xBF16 writes hi/lo operands in the
-//                UMMA MN-major SWIZZLE_128B layout (2-stage staging ring,
-//                2-stage operand ring, the same shared memory);
+//                (2 x ring stages, eight with three staged blocks); 3xBF16
+//                writes hi/lo operands in the UMMA MN-major SWIZZLE_128B
+//                layout (ring staging stages and ring operand stages in the
+//                same shared memory; ring = 4 with three staged blocks);
 //   warps 4-7    also the epilogue (TMEM lane quarters 0-3) at every flush.
 #pragma once
 
@@ -50,9 +51,9 @@ constexpr int kBlock = 128;        // real columns per Gram block (64 complex fr
 constexpr int kRows = 16;          // rows per stage
 constexpr int kMaxLoads = 6;       // staged column blocks per unit
 constexpr int kMaxTasks = 4;       // output blocks per unit (4 x 128 TMEM columns)
-constexpr int kMaxUnits = 40;      // nb <= 16 blocks (T <= 1024): 136 upper blocks -> 34 units
+constexpr int kMaxUnits = 48;      // nb <= 16 blocks (T <= 1024): 136 upper blocks -> 43 units
 constexpr int kMaxBlocks = 16;
-constexpr int kRing = 2;           // 3xBF16 staging and operand ring depth (TF32: one ring of 2 kRing)
+constexpr int kMaxRing = 4;        // deepest 3xBF16 staging and operand rings (TF32: one ring of 2 x ring)
 constexpr int kThreads = 256;
 constexpr int kConverters = 6 * 32;
 constexpr int kSlotBytes = kBlock * kRows * 4;  // 8192: one staged block per stage (f32 or bf16 hi+lo)
@@ -76,6 +77,7 @@ struct Unit {
 
 struct Params {
   int nunits, slices, nload_max, nt;
+  int ring;  // 3xBF16 staging and operand ring depth; TF32 converts in place in one ring of 2 x ring
   long long rows, slice_rows;
   const double* scale;
   double* upper;
@@ -83,8 +85,8 @@ struct Params {
   Unit units[kMaxUnits];
 };
 
-__host__ __device__ inline size_t smem_bytes(int nload_max) {
-  return size_t(2 * kRing) * nload_max * kSlotBytes + 1024 + 1024;
+__host__ __device__ inline size_t smem_bytes(int nload_max, int ring) {
+  return size_t(2 * ring) * nload_max * kSlotBytes + 1024 + 1024;
 }
 
 // kind::tf32 / kind::f16(BF16) instruction descriptor: F32 accumulate, A and B MN-major.
@@ -132,12 +134,12 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc(const __grid_constant__ C
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const Unit& u = p.units[blockIdx.x % p.nunits];
   const int slice = blockIdx.x / p.nunits;
-  // TF32: one 2 kRing-stage ring converted in place; 3xBF16: kRing staging + kRing operand stages.
-  constexpr int R = TF32 ? 2 * kRing : kRing;
+  // TF32: one ring of 2 x ring stages converted in place; 3xBF16: ring staging + ring operand stages.
+  const int R = TF32 ? 2 * p.ring : p.ring;
   const size_t stage_bytes = size_t(p.nload_max) * kSlotBytes;
   unsigned char* staging = smem;
-  unsigned char* operands = TF32 ? smem : smem + kRing * stage_bytes;
-  uint64_t* stg_full = reinterpret_cast<uint64_t*>(smem + 2 * kRing * stage_bytes);
+  unsigned char* operands = TF32 ? smem : smem + p.ring * stage_bytes;
+  uint64_t* stg_full = reinterpret_cast<uint64_t*>(smem + 2 * p.ring * stage_bytes);
   uint64_t* stg_empty = stg_full + R;
   uint64_t* op_full = stg_empty + R;
   uint64_t* op_empty = op_full + R;
@@ -344,45 +346,117 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc(const __grid_constant__ C
   }
 }
 
+inline int unit_slot(const Unit& un, int blk) {
+  for (int j = 0; j < un.nload; ++j)
+    if (un.load[j] == blk) return j;
+  return -1;
+}
+
+// Output (a, b) of a unit, staging blocks a and b if it does not yet.
+inline void unit_add(Unit& un, int a, int b) {
+  if (unit_slot(un, a) < 0) un.load[un.nload++] = a;
+  if (unit_slot(un, b) < 0) un.load[un.nload++] = b;
+  un.a_slot[un.ntask] = unit_slot(un, a);
+  un.b_slot[un.ntask] = unit_slot(un, b);
+  un.a_blk[un.ntask] = a;
+  un.b_blk[un.ntask] = b;
+  ++un.ntask;
+}
+
+// Augmenting path for diagonal block d: a unit among the first n that stages d
+// and has a free output slot, possibly after moving a diagonal it holds on.
+inline bool diagonal_path(int d, int nb, int n, const Unit* units, int* owner, bool* seen) {
+  for (int u = 0; u < n; ++u) {
+    if (seen[u] || unit_slot(units[u], d) < 0) continue;
+    seen[u] = true;
+    int held = 0;
+    for (int e = 0; e < nb; ++e) held += owner[e] == u;
+    if (units[u].ntask + held < kMaxTasks) {
+      owner[d] = u;
+      return true;
+    }
+    for (int e = 0; e < nb; ++e)
+      if (owner[e] == u && diagonal_path(e, nb, n, units, owner, seen)) {
+        owner[d] = u;
+        return true;
+      }
+  }
+  return false;
+}
+
 // Pack the upper 128-column blocks (b <= c) of an nb-block Gram into units of
-// at most four output blocks and six staged blocks; rows b and nb-1-b are
-// taken together so that most units are full.  Returns the unit count, or 0.
+// at most four output blocks (the 512 TMEM columns).  A CTA stages its unit's
+// blocks for every row, so units are built to stage few blocks for their
+// outputs: first edge-disjoint triangles {a, b, c} (three staged blocks for the
+// off-diagonal outputs (a,b), (a,c), (b,c); a Steiner triple system where nb
+// allows, e.g. nb = 7), then the remaining off-diagonal outputs in units of at
+// most three blocks, then each diagonal output (b,b) in a unit that already
+// stages b and has room (augmenting-path matching), the rest in units of up to
+// three diagonals.  At most three staged blocks per unit (T = 400: 7 units of
+// 4 outputs and 21 staged blocks, against 27 when rows b and nb-1-b were
+// paired).  Returns the unit count, or 0.
 inline int plan_units(int nb, Unit* units, int* nload_max) {
   if (nb < 1 || nb > kMaxBlocks) return 0;
-  int seq_a[kMaxBlocks * (kMaxBlocks + 1) / 2], seq_b[kMaxBlocks * (kMaxBlocks + 1) / 2];
-  int n = 0;
-  for (int lo = 0, hi = nb - 1; lo <= hi; ++lo, --hi) {
-    for (int c = lo; c < nb; ++c) seq_a[n] = lo, seq_b[n++] = c;
-    if (hi != lo)
-      for (int c = hi; c < nb; ++c) seq_a[n] = hi, seq_b[n++] = c;
-  }
+  bool open[kMaxBlocks][kMaxBlocks] = {};  // off-diagonal outputs (a < b) not yet in a unit
+  for (int a = 0; a < nb; ++a)
+    for (int b = a + 1; b < nb; ++b) open[a][b] = true;
   int count = 0;
-  *nload_max = 0;
-  for (int i = 0; i < n;) {
-    if (count == kMaxUnits) return 0;
-    Unit& un = units[count++];
-    un.nload = 0;
-    un.ntask = 0;
-    auto slot_of = [&](int blk) {
-      for (int j = 0; j < un.nload; ++j)
-        if (un.load[j] == blk) return j;
-      return -1;
-    };
-    while (i < n && un.ntask < kMaxTasks) {
-      const int a = seq_a[i], b = seq_b[i];
-      const int extra = (slot_of(a) < 0) + (slot_of(b) < 0 && b != a);
-      if (un.nload + extra > kMaxLoads) break;
-      if (slot_of(a) < 0) un.load[un.nload++] = a;
-      if (slot_of(b) < 0) un.load[un.nload++] = b;
-      un.a_slot[un.ntask] = slot_of(a);
-      un.b_slot[un.ntask] = slot_of(b);
-      un.a_blk[un.ntask] = a;
-      un.b_blk[un.ntask] = b;
-      ++un.ntask;
-      ++i;
+  auto fresh = [&]() -> Unit* {
+    if (count == kMaxUnits) return nullptr;
+    Unit* un = &units[count++];
+    un->nload = 0;
+    un->ntask = 0;
+    return un;
+  };
+  // 1. Triangles.
+  for (int a = 0; a < nb; ++a)
+    for (int b = a + 1; b < nb; ++b)
+      for (int c = b + 1; c < nb; ++c) {
+        if (!(open[a][b] && open[a][c] && open[b][c])) continue;
+        Unit* un = fresh();
+        if (!un) return 0;
+        unit_add(*un, a, b);
+        unit_add(*un, a, c);
+        unit_add(*un, b, c);
+        open[a][b] = open[a][c] = open[b][c] = false;
+      }
+  // 2. Remaining off-diagonal outputs, up to three per unit of <= three blocks.
+  for (int a = 0; a < nb; ++a)
+    for (int b = a + 1; b < nb; ++b) {
+      if (!open[a][b]) continue;
+      Unit* un = fresh();
+      if (!un) return 0;
+      unit_add(*un, a, b);
+      open[a][b] = false;
+      for (int c = 0; c < nb && un->ntask < 3; ++c)
+        for (int d = c + 1; d < nb && un->ntask < 3; ++d) {
+          if (!open[c][d] || un->nload + (unit_slot(*un, c) < 0) + (unit_slot(*un, d) < 0) > 3) continue;
+          unit_add(*un, c, d);
+          open[c][d] = false;
+        }
     }
-    if (un.nload > *nload_max) *nload_max = un.nload;
+  // 3. Diagonal outputs into units that stage their block.
+  const int paired = count;
+  int owner[kMaxBlocks];
+  bool seen[kMaxUnits];
+  for (int d = 0; d < nb; ++d) {
+    owner[d] = -1;
+    for (int u = 0; u < paired; ++u) seen[u] = false;
+    diagonal_path(d, nb, paired, units, owner, seen);
   }
+  for (int d = 0; d < nb; ++d)
+    if (owner[d] >= 0) unit_add(units[owner[d]], d, d);
+  // 4. Diagonal outputs left over: up to three per unit.
+  Unit* rest = nullptr;
+  for (int d = 0; d < nb; ++d) {
+    if (owner[d] >= 0) continue;
+    if (!rest || rest->ntask == 3) rest = fresh();
+    if (!rest) return 0;
+    unit_add(*rest, d, d);
+  }
+  *nload_max = 0;
+  for (int u = 0; u < count; ++u)
+    if (units[u].nload > *nload_max) *nload_max = units[u].nload;
   return count;
 }
 

@@ -799,8 +799,13 @@ static rcabeam_status gram_tc_launch(const void* iq, size_t rows, size_t nt, con
          CU_TENSOR_MAP_INTERLEAVE_NONE, tf32 ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B : CU_TENSOR_MAP_SWIZZLE_128B,
          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return RCABEAM_ERROR_ARGUMENT;
-  // At least 120 KB keeps one CTA (and one 512-column TMEM allocation) per SM.
-  const size_t smem = std::max(gramtc::smem_bytes(prm.nload_max), size_t(120) << 10);
+  // The deepest rings that fit 227 KB (units stage at most three blocks: four
+  // 3xBF16 staging and operand stages, eight TF32 stages); at least 120 KB
+  // keeps one CTA (and one 512-column TMEM allocation) per SM.
+  prm.ring = 2;
+  while (prm.ring < gramtc::kMaxRing && gramtc::smem_bytes(prm.nload_max, prm.ring + 1) <= (size_t(227) << 10))
+    ++prm.ring;
+  const size_t smem = std::max(gramtc::smem_bytes(prm.nload_max, prm.ring), size_t(120) << 10);
   auto kern = tf32 ? gramtc::gram_tc<true> : gramtc::gram_tc<false>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
     return RCABEAM_ERROR_CUDA;
