@@ -680,6 +680,132 @@ __global__ void __launch_bounds__(kRegThreads, 3)
   }
 }
 
+// Float64 tensor-core (DMMA, mma.sync m8n8k4 f64) form of the filtered power
+// for complex64 rows with the smaller projector subtracted (mode 1, power
+// only): k <= 4 vectors, nt <= 4 TILES frames.  A warp takes eight rows at a
+// time; lane l holds row r = l / 4 of its group and, for every 4-frame tile j,
+// the complex sample x[r][4 j + l % 4] (one 8-byte load, kept in registers as
+// float).  As real matrices over the interleaved (re, im) components:
+//   Y[8 x 8]  = X[8 x 2T] W1[2T x 8]     (the k complex coordinates, padded)
+//   R[8 x 2T] = X - Y W2[8 x 2T]         (the explicit residual)
+// with the K dimension of the first product ordered so that step 2 j + i gives
+// lane l the component i of its own sample of tile j: the A fragment of every
+// step is a register, and the same registers are the C fragment (X) of the
+// second product's tile j.  W1 and -W2 are laid out in shared memory in
+// fragment order (32 doubles per step), the coordinates move from the first
+// product's D layout to the second's A layout with four shuffles, and each
+// lane adds the squares of its two residual components of every tile.  The
+// float64 work is the register form's (coordinates, residual, squares), in
+// about a tenth of the instructions.
+constexpr int kDmmaThreads = 128;
+constexpr int kDmmaWarps = kDmmaThreads / 32;
+constexpr int kDmmaMaxK = 4;
+
+__host__ __device__ inline size_t dmma_smem_bytes(int tiles) { return size_t(tiles) * 4 * 32 * sizeof(double); }
+
+__device__ __forceinline__ void dmma_f64(double& d0, double& d1, double a, double b, double c0, double c1) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%4, %5};"
+      : "=d"(d0), "=d"(d1)
+      : "d"(a), "d"(b), "d"(c0), "d"(c1));
+}
+
+template <int TILES>
+__global__ void __launch_bounds__(kDmmaThreads, 3)
+    project_power_dmma(const float2* __restrict__ x, double* __restrict__ power, size_t rows, int nt,
+                       const double2* __restrict__ vec, int k, double inv_nt, unsigned* __restrict__ flags) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int tiles = (nt + 3) / 4;
+  double* b1 = reinterpret_cast<double*>(smem);  // [2 tiles][32]: step s = 2 j + i
+  double* b2 = b1 + size_t(tiles) * 2 * 32;     // [tiles][2 k-steps][32]
+  // W1 (step s = 2 j + i, lane l: K row = component i of frame 4 j + l % 4,
+  // N column n = l / 4 = coordinate (n / 2, re / im)):
+  //   yr = sum xr vr - xi vi,  yi = sum xr vi + xi vr.
+  // -W2 (tile j, k-step h, lane l: K row = coordinate component 4 h + l % 4,
+  // N column n = l / 4 = component n % 2 of frame 4 j + n / 2):
+  //   r.re = x.re - (yr vr + yi vi),  r.im = x.im - (yi vr - yr vi).
+  for (int e = threadIdx.x; e < tiles * 2 * 32; e += blockDim.x) {
+    const int s = e >> 5, l = e & 31;
+    {
+      const int j = s >> 1, i = s & 1, t = 4 * j + (l & 3), n = l >> 2, c = n >> 1, pt = n & 1;
+      double w = 0.0;
+      if (t < nt && c < k) {
+        const double2 v = vec[size_t(c) * nt + t];
+        w = i == 0 ? (pt == 0 ? v.x : v.y) : (pt == 0 ? -v.y : v.x);
+      }
+      b1[e] = w;
+    }
+    {
+      const int j = s >> 1, h = s & 1, comp = 4 * h + (l & 3), c = comp >> 1, pc = comp & 1, n = l >> 2;
+      const int t = 4 * j + (n >> 1), o = n & 1;
+      double w = 0.0;
+      if (t < nt && c < k) {
+        const double2 v = vec[size_t(c) * nt + t];
+        w = o == 0 ? (pc == 0 ? -v.x : -v.y) : (pc == 0 ? v.y : -v.x);
+      }
+      b2[e] = w;
+    }
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, q = lane & 3;
+  const size_t groups = (rows + 7) / 8;
+  bool bad_in = false, bad_out = false;
+  for (size_t g = size_t(blockIdx.x) * kDmmaWarps + warp; g < groups; g += size_t(gridDim.x) * kDmmaWarps) {
+    const size_t r = 8 * g + (lane >> 2);
+    const bool live = r < rows;
+    const float2* row = x + r * size_t(nt);
+    float2 xs[TILES];
+#pragma unroll
+    for (int j = 0; j < TILES; ++j) {
+      const int t = 4 * j + q;
+      xs[j] = (j < tiles && live && t < nt) ? row[t] : make_float2(0.f, 0.f);
+      bad_in |= !isfinite(xs[j].x) || !isfinite(xs[j].y);
+    }
+    // Y = X W1, in four partial accumulators (independent chains).
+    double y[4][2] = {};
+#pragma unroll
+    for (int j = 0; j < TILES; ++j) {
+      if (j < tiles) {
+        dmma_f64(y[(2 * j) & 3][0], y[(2 * j) & 3][1], double(xs[j].x), b1[(2 * j) * 32 + lane],
+                 y[(2 * j) & 3][0], y[(2 * j) & 3][1]);
+        dmma_f64(y[(2 * j + 1) & 3][0], y[(2 * j + 1) & 3][1], double(xs[j].y), b1[(2 * j + 1) * 32 + lane],
+                 y[(2 * j + 1) & 3][0], y[(2 * j + 1) & 3][1]);
+      }
+    }
+    // Lane l holds Y[r][2 q], Y[r][2 q + 1] (coordinate q: re, im).
+    const double y0 = (y[0][0] + y[1][0]) + (y[2][0] + y[3][0]);
+    const double y1 = (y[0][1] + y[1][1]) + (y[2][1] + y[3][1]);
+    // A fragments of R = X - Y W2: step h needs component 4 h + q of row r.
+    double a[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int src = (lane & ~3) + 2 * h + (q >> 1);
+      const double s0 = __shfl_sync(0xffffffffu, y0, src), s1 = __shfl_sync(0xffffffffu, y1, src);
+      a[h] = (q & 1) ? s1 : s0;
+    }
+    double pw[2] = {0.0, 0.0};
+#pragma unroll
+    for (int j = 0; j < TILES; ++j) {
+      if (j < tiles) {
+        double d0, d1;
+        dmma_f64(d0, d1, a[0], b2[(2 * j) * 32 + lane], double(xs[j].x), double(xs[j].y));
+        dmma_f64(d0, d1, a[1], b2[(2 * j + 1) * 32 + lane], d0, d1);
+        pw[j & 1] = fma(d0, d0, fma(d1, d1, pw[j & 1]));
+      }
+    }
+    double p = pw[0] + pw[1];
+    p += __shfl_xor_sync(0xffffffffu, p, 1);
+    p += __shfl_xor_sync(0xffffffffu, p, 2);
+    if (q == 0 && live) {
+      power[r] = p * inv_nt;
+      bad_out |= !isfinite(p);
+    }
+  }
+  if (flags) {
+    const unsigned bits = (__any_sync(0xffffffffu, bad_in) ? 1u : 0u) | (__any_sync(0xffffffffu, bad_out) ? 2u : 0u);
+    if (bits && lane == 0) atomicOr(flags, bits);
+  }
+}
+
 // The flags of project_rows_async for the other projection kernels: bit 0 for
 // a non-finite input component, bit 1 for a non-finite power (when given).
 template <typename IN>

@@ -604,6 +604,39 @@ static void launch_reg(const void* iq, void* out, double* power, size_t rows, si
                                                         mode, 1.0 / double(nt), flags);
 }
 
+template <int TILES>
+static void launch_dmma(const void* iq, double* power, size_t rows, size_t nt, const double* vec, size_t k,
+                        unsigned* flags) {
+  auto kern = clutter::project_power_dmma<TILES>;
+  const int tiles = int((nt + 3) / 4);
+  const size_t smem = clutter::dmma_smem_bytes(tiles);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  int dev = 0, sms = 148, per_sm = 3;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, clutter::kDmmaThreads, smem);
+  const size_t groups = (rows + 7) / 8;
+  const size_t want = (groups + clutter::kDmmaWarps - 1) / clutter::kDmmaWarps;
+  const size_t grid = std::min(want, size_t(sms) * size_t(per_sm > 0 ? per_sm : 1));
+  kern<<<unsigned(grid), clutter::kDmmaThreads, smem>>>(static_cast<const float2*>(iq), power, rows, int(nt),
+                                                         reinterpret_cast<const double2*>(vec), int(k),
+                                                         1.0 / double(nt), flags);
+}
+
+// Complex64 filtered power with the smaller projector subtracted (mode 1, no
+// filtered IQ), 1-4 vectors, 33-256 frames: the float64 tensor-core form.
+static bool project_dmma(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
+                         size_t k, int mode, unsigned* flags) {
+  if (mode != 1 || out || !power || k < 1 || k > size_t(clutter::kDmmaMaxK) || nt <= 32 || nt > 256) return false;
+  const size_t tiles = (nt + 3) / 4;
+  if (tiles <= 16) launch_dmma<16>(iq, power, rows, nt, vec, k, flags);
+  else if (tiles <= 32) launch_dmma<32>(iq, power, rows, nt, vec, k, flags);
+  else if (tiles <= 48) launch_dmma<48>(iq, power, rows, nt, vec, k, flags);
+  else if (tiles <= 56) launch_dmma<56>(iq, power, rows, nt, vec, k, flags);
+  else launch_dmma<64>(iq, power, rows, nt, vec, k, flags);
+  return true;
+}
+
 // Complex64, 1-3 vectors, 33-512 frames: the register form (a warp pair per
 // row above 256 frames).
 static bool project_reg(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
@@ -624,6 +657,7 @@ template <typename IN>
 static void project_dispatch(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
                              size_t k, int mode, unsigned* flags) {
   if constexpr (sizeof(IN) == 8) {
+    if (project_dmma(iq, out, power, rows, nt, vec, k, mode, flags)) return;
     if (project_reg(iq, out, power, rows, nt, vec, k, mode, flags)) return;
   }
   if (k <= size_t(clutter::kProjSmall)) {

@@ -55,7 +55,9 @@ def _fro(a, b):
 
 @pytest.mark.parametrize("precision", ["tf32", "bf16x3"])
 @pytest.mark.parametrize("rows,frames", [(1, 2), (37, 16), (1000, 64), (5003, 66), (40000, 200), (2048, 400),
-                                         (777, 1024)])
+                                         (777, 1024),
+                                         # every unit shape of the block planner: 3, 5, 6, 8, 10, 13 blocks
+                                         (300, 130), (300, 320), (300, 384), (300, 512), (200, 600), (200, 832)])
 def test_gram_matches_float64(precision, rows, frames):
     rng = np.random.default_rng(rows + frames)
     host = (rng.normal(size=(rows, frames)) + 1j * rng.normal(size=(rows, frames))).astype(np.complex64)
