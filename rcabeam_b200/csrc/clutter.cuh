@@ -680,25 +680,25 @@ __global__ void __launch_bounds__(kRegThreads, 3)
   }
 }
 
-// Float64 tensor-core (DMMA, mma.sync m8n8k4 f64) form of the filtered power
-// for complex64 rows with the smaller projector subtracted (mode 1, power
-// only): k <= 4 vectors, nt <= 4 TILES frames.  A warp takes eight rows at a
-// time; lane l holds row r = l / 4 of its group and, for every 4-frame tile j,
-// the complex sample x[r][4 j + l % 4] (one 8-byte load, kept in registers as
-// float).  As real matrices over the interleaved (re, im) components:
+// Float64 tensor-core (DMMA, mma.sync m8n8k4 f64) filtered power for
+// complex64 rows with the smaller projector subtracted (mode 1, power only):
+// k <= 4 vectors, nt <= 512 frames.  A warp takes eight rows at a time; lane
+// l works on row r = l / 4 of its group and, for every 4-frame tile j, on the
+// complex sample x[r][4 j + l % 4] (one 8-byte load).  As real matrices over
+// the interleaved (re, im) components:
 //   Y[8 x 8]  = X[8 x 2T] W1[2T x 8]     (the k complex coordinates, padded)
 //   R[8 x 2T] = X - Y W2[8 x 2T]         (the explicit residual)
 // with the K dimension of the first product ordered so that step 2 j + i gives
-// lane l the component i of its own sample of tile j: the A fragment of every
-// step is a register, and the same registers are the C fragment (X) of the
-// second product's tile j.  W1 and -W2 are laid out in shared memory in
-// fragment order (32 doubles per step), the coordinates move from the first
-// product's D layout to the second's A layout with four shuffles, and each
-// lane adds the squares of its two residual components of every tile.  The
-// float64 work is the register form's (coordinates, residual, squares), in
-// about a tenth of the instructions.
-constexpr int kDmmaThreads = 128;
-constexpr int kDmmaWarps = kDmmaThreads / 32;
+// lane l the component i of its own sample of tile j: each loaded sample is
+// the A fragment of two steps of the first product and, read again, the C
+// fragment (X) of the second product's tile j.  W1 and -W2 are laid out in
+// shared memory in fragment order (32 doubles per step), the coordinates move
+// from the first product's D layout to the second's A layout with four
+// shuffles, and each lane adds the squares of its two residual components of
+// every tile.  The float64 work is the register form's (coordinates, residual,
+// squares) in about a tenth of the instructions.  Samples are read in batches
+// of B tiles, the next batch in flight while the current one is multiplied;
+// the second read is served by L1 / L2.  8 warps per CTA share the tables.
 constexpr int kDmmaMaxK = 4;
 
 __host__ __device__ inline size_t dmma_smem_bytes(int tiles) { return size_t(tiles) * 4 * 32 * sizeof(double); }
@@ -709,8 +709,11 @@ __device__ __forceinline__ void dmma_f64(double& d0, double& d1, double a, doubl
       : "d"(a), "d"(b), "d"(c0), "d"(c1));
 }
 
-template <int TILES>
-__global__ void __launch_bounds__(kDmmaThreads, 3)
+constexpr int kDmmaThreads = 256;
+constexpr int kDmmaWarps = kDmmaThreads / 32;
+
+template <int B>
+__global__ void __launch_bounds__(kDmmaThreads, 2)
     project_power_dmma(const float2* __restrict__ x, double* __restrict__ power, size_t rows, int nt,
                        const double2* __restrict__ vec, int k, double inv_nt, unsigned* __restrict__ flags) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -749,32 +752,40 @@ __global__ void __launch_bounds__(kDmmaThreads, 3)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, q = lane & 3;
   const size_t groups = (rows + 7) / 8;
   bool bad_in = false, bad_out = false;
-  for (size_t g = size_t(blockIdx.x) * kDmmaWarps + warp; g < groups; g += size_t(gridDim.x) * kDmmaWarps) {
+  for (size_t g = size_t(blockIdx.x) * kDmmaWarps + warp; g < groups;
+       g += size_t(gridDim.x) * kDmmaWarps) {
     const size_t r = 8 * g + (lane >> 2);
     const bool live = r < rows;
     const float2* row = x + r * size_t(nt);
-    float2 xs[TILES];
-#pragma unroll
-    for (int j = 0; j < TILES; ++j) {
+    auto load = [&](int j) {
       const int t = 4 * j + q;
-      xs[j] = (j < tiles && live && t < nt) ? row[t] : make_float2(0.f, 0.f);
-      bad_in |= !isfinite(xs[j].x) || !isfinite(xs[j].y);
-    }
-    // Y = X W1, in four partial accumulators (independent chains).
-    double y[4][2] = {};
+      return (j < tiles && live && t < nt) ? row[t] : make_float2(0.f, 0.f);
+    };
+    float2 cur[B], nxt[B];
 #pragma unroll
-    for (int j = 0; j < TILES; ++j) {
-      if (j < tiles) {
-        dmma_f64(y[(2 * j) & 3][0], y[(2 * j) & 3][1], double(xs[j].x), b1[(2 * j) * 32 + lane],
-                 y[(2 * j) & 3][0], y[(2 * j) & 3][1]);
-        dmma_f64(y[(2 * j + 1) & 3][0], y[(2 * j + 1) & 3][1], double(xs[j].y), b1[(2 * j + 1) * 32 + lane],
-                 y[(2 * j + 1) & 3][0], y[(2 * j + 1) & 3][1]);
+    for (int i = 0; i < B; ++i) cur[i] = load(i);
+    double y[4][2] = {};
+    for (int jb = 0; jb < tiles; jb += B) {
+#pragma unroll
+      for (int i = 0; i < B; ++i) nxt[i] = load(jb + B + i);
+#pragma unroll
+      for (int i = 0; i < B; ++i) {
+        const int j = jb + i;
+        if (j < tiles) {
+          bad_in |= !isfinite(cur[i].x) || !isfinite(cur[i].y);
+          dmma_f64(y[(2 * i) & 3][0], y[(2 * i) & 3][1], double(cur[i].x), b1[(2 * j) * 32 + lane],
+                   y[(2 * i) & 3][0], y[(2 * i) & 3][1]);
+          dmma_f64(y[(2 * i + 1) & 3][0], y[(2 * i + 1) & 3][1], double(cur[i].y), b1[(2 * j + 1) * 32 + lane],
+                   y[(2 * i + 1) & 3][0], y[(2 * i + 1) & 3][1]);
+        }
       }
+#pragma unroll
+      for (int i = 0; i < B; ++i) cur[i] = nxt[i];
     }
-    // Lane l holds Y[r][2 q], Y[r][2 q + 1] (coordinate q: re, im).
+    // Lane l holds Y[r][2 q], Y[r][2 q + 1] (coordinate q: re, im); the A
+    // fragment of k-step h of R = X - Y W2 is component 4 h + q of row r.
     const double y0 = (y[0][0] + y[1][0]) + (y[2][0] + y[3][0]);
     const double y1 = (y[0][1] + y[1][1]) + (y[2][1] + y[3][1]);
-    // A fragments of R = X - Y W2: step h needs component 4 h + q of row r.
     double a[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -784,13 +795,22 @@ __global__ void __launch_bounds__(kDmmaThreads, 3)
     }
     double pw[2] = {0.0, 0.0};
 #pragma unroll
-    for (int j = 0; j < TILES; ++j) {
-      if (j < tiles) {
-        double d0, d1;
-        dmma_f64(d0, d1, a[0], b2[(2 * j) * 32 + lane], double(xs[j].x), double(xs[j].y));
-        dmma_f64(d0, d1, a[1], b2[(2 * j + 1) * 32 + lane], d0, d1);
-        pw[j & 1] = fma(d0, d0, fma(d1, d1, pw[j & 1]));
+    for (int i = 0; i < B; ++i) cur[i] = load(i);
+    for (int jb = 0; jb < tiles; jb += B) {
+#pragma unroll
+      for (int i = 0; i < B; ++i) nxt[i] = load(jb + B + i);
+#pragma unroll
+      for (int i = 0; i < B; ++i) {
+        const int j = jb + i;
+        if (j < tiles) {
+          double d0, d1;
+          dmma_f64(d0, d1, a[0], b2[(2 * j) * 32 + lane], double(cur[i].x), double(cur[i].y));
+          dmma_f64(d0, d1, a[1], b2[(2 * j + 1) * 32 + lane], d0, d1);
+          pw[i & 1] = fma(d0, d0, fma(d1, d1, pw[i & 1]));
+        }
       }
+#pragma unroll
+      for (int i = 0; i < B; ++i) cur[i] = nxt[i];
     }
     double p = pw[0] + pw[1];
     p += __shfl_xor_sync(0xffffffffu, p, 1);

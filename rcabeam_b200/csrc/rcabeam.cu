@@ -604,14 +604,12 @@ static void launch_reg(const void* iq, void* out, double* power, size_t rows, si
                                                         mode, 1.0 / double(nt), flags);
 }
 
-template <int TILES>
 static void launch_dmma(const void* iq, double* power, size_t rows, size_t nt, const double* vec, size_t k,
                         unsigned* flags) {
-  auto kern = clutter::project_power_dmma<TILES>;
-  const int tiles = int((nt + 3) / 4);
-  const size_t smem = clutter::dmma_smem_bytes(tiles);
+  auto kern = clutter::project_power_dmma<8>;
+  const size_t smem = clutter::dmma_smem_bytes(int((nt + 3) / 4));
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  int dev = 0, sms = 148, per_sm = 3;
+  int dev = 0, sms = 148, per_sm = 2;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, clutter::kDmmaThreads, smem);
@@ -624,16 +622,11 @@ static void launch_dmma(const void* iq, double* power, size_t rows, size_t nt, c
 }
 
 // Complex64 filtered power with the smaller projector subtracted (mode 1, no
-// filtered IQ), 1-4 vectors, 33-256 frames: the float64 tensor-core form.
+// filtered IQ), 1-4 vectors, 33-512 frames: the float64 tensor-core form.
 static bool project_dmma(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
                          size_t k, int mode, unsigned* flags) {
-  if (mode != 1 || out || !power || k < 1 || k > size_t(clutter::kDmmaMaxK) || nt <= 32 || nt > 256) return false;
-  const size_t tiles = (nt + 3) / 4;
-  if (tiles <= 16) launch_dmma<16>(iq, power, rows, nt, vec, k, flags);
-  else if (tiles <= 32) launch_dmma<32>(iq, power, rows, nt, vec, k, flags);
-  else if (tiles <= 48) launch_dmma<48>(iq, power, rows, nt, vec, k, flags);
-  else if (tiles <= 56) launch_dmma<56>(iq, power, rows, nt, vec, k, flags);
-  else launch_dmma<64>(iq, power, rows, nt, vec, k, flags);
+  if (mode != 1 || out || !power || k < 1 || k > size_t(clutter::kDmmaMaxK) || nt <= 32 || nt > 512) return false;
+  launch_dmma(iq, power, rows, nt, vec, k, flags);
   return true;
 }
 
