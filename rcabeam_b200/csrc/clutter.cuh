@@ -698,7 +698,8 @@ __global__ void __launch_bounds__(kRegThreads, 3)
 // every tile.  The float64 work is the register form's (coordinates, residual,
 // squares) in about a tenth of the instructions.  Samples are read in batches
 // of B tiles, the next batch in flight while the current one is multiplied;
-// the second read is served by L1 / L2.  8 warps per CTA share the tables.
+// the second read is served by L1 / L2.  8 warps per CTA share the tables;
+// at most 85 registers, so three CTAs fit an SM where the tables allow.
 constexpr int kDmmaMaxK = 4;
 
 __host__ __device__ inline size_t dmma_smem_bytes(int tiles) { return size_t(tiles) * 4 * 32 * sizeof(double); }
@@ -713,7 +714,7 @@ constexpr int kDmmaThreads = 256;
 constexpr int kDmmaWarps = kDmmaThreads / 32;
 
 template <int B>
-__global__ void __launch_bounds__(kDmmaThreads, 2)
+__global__ void __launch_bounds__(kDmmaThreads, 3)
     project_power_dmma(const float2* __restrict__ x, double* __restrict__ power, size_t rows, int nt,
                        const double2* __restrict__ vec, int k, double inv_nt, unsigned* __restrict__ flags) {
   extern __shared__ __align__(16) unsigned char smem[];
