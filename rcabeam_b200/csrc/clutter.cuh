@@ -680,9 +680,10 @@ __global__ void __launch_bounds__(kRegThreads, 3)
   }
 }
 
-// Float64 tensor-core (DMMA, mma.sync m8n8k4 f64) filtered power for
-// complex64 rows with the smaller projector subtracted (mode 1, power only):
-// k <= 4 vectors, nt <= 512 frames.  A warp takes eight rows at a time; lane
+// Float64 tensor-core (DMMA, mma.sync m8n8k4 f64) filtered power and filtered
+// IQ for complex64 rows with the smaller projector subtracted (mode 1: power;
+// mode 3: the residual written to out, power optional): k <= 4 vectors,
+// nt <= 512 frames.  A warp takes eight rows at a time; lane
 // l works on row r = l / 4 of its group and, for every 4-frame tile j, on the
 // complex sample x[r][4 j + l % 4] (one 8-byte load).  As real matrices over
 // the interleaved (re, im) components:
@@ -715,8 +716,9 @@ constexpr int kDmmaWarps = kDmmaThreads / 32;
 
 template <int B>
 __global__ void __launch_bounds__(kDmmaThreads, 3)
-    project_power_dmma(const float2* __restrict__ x, double* __restrict__ power, size_t rows, int nt,
-                       const double2* __restrict__ vec, int k, double inv_nt, unsigned* __restrict__ flags) {
+    project_power_dmma(const float2* __restrict__ x, float2* __restrict__ out, double* __restrict__ power,
+                       size_t rows, int nt, const double2* __restrict__ vec, int k, double inv_nt,
+                       unsigned* __restrict__ flags) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int tiles = (nt + 3) / 4;
   double* b1 = reinterpret_cast<double*>(smem);  // [2 tiles][32]: step s = 2 j + i
@@ -808,6 +810,7 @@ __global__ void __launch_bounds__(kDmmaThreads, 3)
           dmma_f64(d0, d1, a[0], b2[(2 * j) * 32 + lane], double(cur[i].x), double(cur[i].y));
           dmma_f64(d0, d1, a[1], b2[(2 * j + 1) * 32 + lane], d0, d1);
           pw[i & 1] = fma(d0, d0, fma(d1, d1, pw[i & 1]));
+          if (out && live && 4 * j + q < nt) out[r * size_t(nt) + 4 * j + q] = make_float2(float(d0), float(d1));
         }
       }
 #pragma unroll
@@ -816,7 +819,7 @@ __global__ void __launch_bounds__(kDmmaThreads, 3)
     double p = pw[0] + pw[1];
     p += __shfl_xor_sync(0xffffffffu, p, 1);
     p += __shfl_xor_sync(0xffffffffu, p, 2);
-    if (q == 0 && live) {
+    if (power && q == 0 && live) {
       power[r] = p * inv_nt;
       bad_out |= !isfinite(p);
     }

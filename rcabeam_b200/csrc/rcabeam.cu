@@ -604,8 +604,8 @@ static void launch_reg(const void* iq, void* out, double* power, size_t rows, si
                                                         mode, 1.0 / double(nt), flags);
 }
 
-static void launch_dmma(const void* iq, double* power, size_t rows, size_t nt, const double* vec, size_t k,
-                        unsigned* flags) {
+static void launch_dmma(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
+                        size_t k, unsigned* flags) {
   auto kern = clutter::project_power_dmma<8>;
   const size_t smem = clutter::dmma_smem_bytes(int((nt + 3) / 4));
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
@@ -616,17 +616,20 @@ static void launch_dmma(const void* iq, double* power, size_t rows, size_t nt, c
   const size_t groups = (rows + 7) / 8;
   const size_t want = (groups + clutter::kDmmaWarps - 1) / clutter::kDmmaWarps;
   const size_t grid = std::min(want, size_t(sms) * size_t(per_sm > 0 ? per_sm : 1));
-  kern<<<unsigned(grid), clutter::kDmmaThreads, smem>>>(static_cast<const float2*>(iq), power, rows, int(nt),
+  kern<<<unsigned(grid), clutter::kDmmaThreads, smem>>>(static_cast<const float2*>(iq), static_cast<float2*>(out),
+                                                         power, rows, int(nt),
                                                          reinterpret_cast<const double2*>(vec), int(k),
                                                          1.0 / double(nt), flags);
 }
 
-// Complex64 filtered power with the smaller projector subtracted (mode 1, no
-// filtered IQ), 1-4 vectors, 33-512 frames: the float64 tensor-core form.
+// Complex64 rows with the smaller projector subtracted, 1-4 vectors, 33-512
+// frames: the float64 tensor-core form (mode 1: filtered power; mode 3: the
+// filtered IQ, power optional).
 static bool project_dmma(const void* iq, void* out, double* power, size_t rows, size_t nt, const double* vec,
                          size_t k, int mode, unsigned* flags) {
-  if (mode != 1 || out || !power || k < 1 || k > size_t(clutter::kDmmaMaxK) || nt <= 32 || nt > 512) return false;
-  launch_dmma(iq, power, rows, nt, vec, k, flags);
+  const bool power_only = mode == 1 && power, residual = mode == 3 && out;
+  if (!(power_only || residual) || k < 1 || k > size_t(clutter::kDmmaMaxK) || nt <= 32 || nt > 512) return false;
+  launch_dmma(iq, residual ? out : nullptr, power, rows, nt, vec, k, flags);
   return true;
 }
 
