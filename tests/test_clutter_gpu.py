@@ -378,3 +378,55 @@ def test_filtered_power_and_basis_reject_non_finite_input():
         for precision in ("complex128", "bf16x3"):
             with pytest.raises(ValueError, match="finite"):
                 gpu_clutter.temporal_basis(y, precision=precision)
+
+
+def _project_case(rows, frames, k, seed):
+    rng = np.random.default_rng(seed)
+    x = (rng.normal(size=(rows, frames)) + 1j * rng.normal(size=(rows, frames))).astype(np.complex64)
+    x[:, :] *= np.exp(rng.normal(size=(rows, 1)))  # row scales over a few orders of magnitude
+    q, _ = np.linalg.qr(rng.normal(size=(frames, k)) + 1j * rng.normal(size=(frames, k)))
+    return x, q  # q: (frames, k) orthonormal columns
+
+
+@pytest.mark.parametrize("frames", [33, 37, 64, 201, 256, 257, 400, 511, 512])
+@pytest.mark.parametrize("k", [1, 3, 4])
+def test_projection_residual_against_float64(frames, k):
+    """rcabeam_project_device with the smaller projector subtracted (the float64
+    tensor-core form for complex64 rows, k <= 4, 33-512 frames): power (mode 1) and
+    filtered IQ (mode 3) against x - (x V) V^H in complex128 (gpu_clutter.py:212-273),
+    on 1001 rows (not a multiple of the 8-row tiles) and frame counts off the 4-frame
+    tiles."""
+    x, v = _project_case(1001, frames, k, seed=frames * 10 + k)
+    xd = x.astype(np.complex128)
+    resid = xd - (xd @ v) @ v.conj().T
+    want_pw = np.sum(np.abs(resid) ** 2, axis=1) / frames
+    dx = _dev(x)
+    vec = _dev(np.ascontiguousarray(v.T))  # (k, frames): vector c in row c
+    power = torch.empty(x.shape[0], dtype=torch.float64, device="cuda")
+    flags = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _lib.call("rcabeam_project_device", dx.data_ptr(), None, power.data_ptr(), x.shape[0], frames, 0, vec.data_ptr(),
+              k, 1, flags.data_ptr())
+    np.testing.assert_allclose(power.cpu().numpy(), want_pw, rtol=1e-12, atol=0)
+    out = torch.empty_like(dx)
+    _lib.call("rcabeam_project_device", dx.data_ptr(), out.data_ptr(), None, x.shape[0], frames, 0, vec.data_ptr(),
+              k, 3, flags.data_ptr())
+    got = out.cpu().numpy()
+    # complex64 rounding of the residual (relative to each row's magnitude)
+    scale = np.abs(xd).max(axis=1, keepdims=True)
+    assert np.max(np.abs(got - resid) / scale) <= 2e-7
+    assert int(flags.item()) == 0
+
+
+def test_projection_flags_non_finite_rows():
+    """A non-finite input component sets flag bit 0 and its non-finite power bit 1."""
+    x, v = _project_case(64, 200, 3, seed=5)
+    x[17, 101] = np.nan
+    dx = _dev(x)
+    vec = _dev(np.ascontiguousarray(v.T))
+    power = torch.empty(x.shape[0], dtype=torch.float64, device="cuda")
+    flags = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _lib.call("rcabeam_project_device", dx.data_ptr(), None, power.data_ptr(), x.shape[0], 200, 0, vec.data_ptr(),
+              3, 1, flags.data_ptr())
+    assert int(flags.item()) == 3
+    pw = power.cpu().numpy()
+    assert not np.isfinite(pw[17]) and np.isfinite(np.delete(pw, 17)).all()
